@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of LAMB's sector multiply C = A.B on B200.
+
+Workload (default): 6144 waters (18,432 atoms, O block 13 / H block 5,
+matrix dimension 141,312) in a 56.8 A periodic box, cutoff 8 A, A and B from
+seeds 1 and 2, eps 1e-10, synthetic (seeded generator, include/lamb_gen.h).
+One step = one full multiply (symbolic phase + numeric phase + result filter)
+on inputs resident in HBM.  The inputs (1.9 GB each) exceed the 126 MB L2, so
+no flush is needed between steps.
+
+Printed JSON line (rank 0): metric GFLOP/s (FP64-equivalent flops counted
+from the block pattern: sum of 2*b_i*b_k*b_j over executed products), the
+dominant kernel's roofline against the FP64 tensor-pipe peak measured live on
+the same GPU, the whole multiply's fraction of the measured HBM copy
+bandwidth, the end-to-end number through the C ABI with host buffers, and the
+CPU baseline (the oracle restatement on a bounded row sample).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank runs an independent replica (nothing in the
+multiply shards at one rank); value is the sum over ranks of flops divided by
+the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "block-SpGEMM GFLOP/s (FP64-equivalent), LAMB sector multiply"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="water6144_cut8", choices=["water6144_cut8", "water192_cut6"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    return p.parse_args()
+
+
+def workload(name):
+    from lamb_b200 import gen
+    return {"water6144_cut8": gen.WATER_6144, "water192_cut6": gen.WATER_192}[name]
+
+
+def algorithmic_bytes(a, b, c) -> int:
+    """Compulsory bytes of one multiply: FP64 elements of A, B, C plus the
+    index (row_p 8 B per row, col_i 2 B and extents 16 B per block)."""
+    tot = 0
+    for m in (a, b, c):
+        for s in m.sectors:
+            used = int((s.extents[:, 1] - s.extents[:, 0] + 1).sum()) if s.n_blks else 0
+            tot += 8 * used + 8 * (s.n_rows + 1) + 18 * s.n_blks
+    return tot
+
+
+class Clocks:
+    """nvidia-smi sampler (200 ms) over the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def committed_traffic(kernel, wl):
+    path = os.path.join(REPO, "profiles", f"{kernel}_{wl}.traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def cpu_sample(a, b, eps, seconds, threads):
+    """Times the oracle on every s-th C row, s picked for about `seconds`."""
+    import oracle
+    probe = 997
+    t = time.perf_counter()
+    _, st = oracle.multiply(a, b, eps, threads=threads, row_stride=probe)
+    dt = max(time.perf_counter() - t, 1e-3)
+    stride = max(1, int(probe * dt / seconds))
+    t = time.perf_counter()
+    c, st = oracle.multiply(a, b, eps, threads=threads, row_stride=stride)
+    dt = time.perf_counter() - t
+    return c, st, dt, stride
+
+
+def rows_of(m, stride):
+    out = {}
+    for s in m.sectors:
+        rows = s.block_rows()
+        for bi in range(s.n_blks):
+            r = int(rows[bi])
+            if r % stride == 0:
+                f, l = int(s.extents[bi, 0]), int(s.extents[bi, 1])
+                out[(s.subset_row, s.subset_col, r, int(s.col_i[bi]))] = s.data[f - 1:l]
+    return out
+
+
+def sampled_error(c_gpu, c_ref, stride):
+    import numpy as np
+    g, r = rows_of(c_gpu, stride), rows_of(c_ref, stride)
+    if set(g) != set(r):
+        return float("inf")
+    num = sum(float(np.sum((g[k] - r[k]) ** 2)) for k in r)
+    den = sum(float(np.sum(r[k] ** 2)) for k in r)
+    return float(np.sqrt(num / den)) if den > 0 else 0.0
+
+
+def pin_matrix(m):
+    """Copies a host matrix into page-locked buffers (the e2e inputs)."""
+    import numpy as np
+    import torch
+    from lamb_b200.matrix import LambMatrix, Sector
+    keep = []
+
+    def pin(x):
+        t = torch.empty(x.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(x.dtype).reshape(x.shape)
+        v[...] = x
+        keep.append(t)
+        return v
+    secs = [Sector(s.subset_row, s.subset_col, pin(s.row_blk_sizes), pin(s.col_blk_sizes), pin(s.row_p),
+                   pin(s.col_i), pin(s.extents), pin(s.data)) for s in m.sectors]
+    out = LambMatrix(secs, m.name)
+    out._keep = keep
+    return out
+
+
+def matrix_bytes(m):
+    return sum(x.nbytes for s in m.sectors for x in (s.row_blk_sizes, s.col_blk_sizes, s.row_p, s.col_i,
+                                                      s.extents, s.data))
+
+
+def run_reference(args):
+    """CPU arm: the oracle (the reference's multiply is a stub and its Fortran
+    does not build here), all host cores, a bounded row sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = workload(args.workload)
+    g, a, b = wl.build()
+    threads = os.cpu_count() or 1
+    per_step = max(2.0, min(20.0, 150.0 / max(args.steps + args.warmup, 1)))
+    import oracle
+    _, _, dt, stride = cpu_sample(a, b, wl.eps, per_step, threads)
+    for _ in range(args.warmup):
+        oracle.multiply(a, b, wl.eps, threads=threads, row_stride=stride)
+    fl, tt = 0.0, 0.0
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        _, st = oracle.multiply(a, b, wl.eps, threads=threads, row_stride=stride)
+        tt += time.perf_counter() - t
+        fl += st["flops"]
+    v = fl / tt / 1e9
+    sample = f"every {stride}-th C block row of {wl.name} per step"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "n_mol": wl.n_mol, "box": wl.box, "cutoff": wl.cutoff, "eps": wl.eps},
+            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "oracle restatement (the reference's sector_multiply is a stub and needs gfortran+MPI)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from lamb_b200 import build, gpu
+    build.build_all()
+    from lamb_b200.gpu import Context
+    import ctypes
+    wl = workload(args.workload)
+    g, a, b = wl.build()
+    ctx = Context(local)
+    lib = gpu.lib()
+    lib.lamb_probe_fp64_tflops.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+    peak = ctypes.c_double()
+    ctx.check(lib.lamb_probe_fp64_tflops(local, 5, ctypes.byref(peak)))
+    fp64_peak = peak.value
+    da, db = ctx.upload(a), ctx.upload(b)
+    dc = ctx.create_like(da)
+    ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local))
+    for _ in range(args.warmup):
+        st = ctx.multiply(da, db, dc, wl.eps)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = Clocks(local)
+    with torch.cuda.stream(ext):
+        e0.record()
+    stats = []
+    for _ in range(args.steps):
+        stats.append(ctx.multiply(da, db, dc, wl.eps))
+    with torch.cuda.stream(ext):
+        e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    flops = stats[-1]["flops"]
+    value = flops * args.steps * world / (ms_max * 1e-3) / 1e9
+    ms_num = statistics.mean(s["ms_numeric"] for s in stats)
+    ms_tot = statistics.mean(s["ms_total"] for s in stats)
+    c_host = dc.download()
+    alg_bytes = algorithmic_bytes(a, b, c_host)
+    peaks, peak_kind = measured_peaks()
+    achieved_tf = flops / (ms_num * 1e-3) / 1e12
+    # e2e through the C ABI with page-locked host buffers
+    pa, pb = pin_matrix(a), pin_matrix(b)
+    c_out = dc.download(pinned=True)
+    h2d = matrix_bytes(pa) + matrix_bytes(pb)
+    d2h = matrix_bytes(c_out)
+    barrier()
+    t_e2e = []
+    for _ in range(max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        xa, xb = ctx.upload(pa), ctx.upload(pb)
+        xc = ctx.create_like(xa)
+        st_e = ctx.multiply(xa, xb, xc, wl.eps)
+        c_out = xc.download(out=c_out)
+        xc.destroy(); xb.destroy(); xa.destroy()
+        t_e2e.append(time.perf_counter() - t)
+    e2e_t = torch.tensor([statistics.mean(t_e2e)], device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = flops * world / float(e2e_t.item()) / 1e9
+    cpu = None
+    err = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        c_ref, st_ref, dt, stride = cpu_sample(a, b, wl.eps, args.cpu_seconds, threads)
+        cpu = {"value": st_ref["flops"] / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+               "sample": f"every {stride}-th C block row of {wl.name} ({st_ref['flops'] / 1e9:.1f} GFLOP, "
+                         f"{dt:.1f} s)"}
+        err = sampled_error(c_host, c_ref, stride)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water boxes)",
+            "config": {"workload": wl.name, "n_mol": wl.n_mol, "n_atoms": g.n_atoms, "box": wl.box,
+                       "cutoff": wl.cutoff, "eps": wl.eps, "path": "plain FP64 (DMMA)",
+                       "l2": "inputs 2x1.9 GB exceed L2; no flush", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "tensor", "kernel": "k_numeric_fp64", "achieved": achieved_tf,
+                         "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak,
+                         "peak_source": "FP64 DMMA probe measured on this GPU in this run",
+                         "traffic": committed_traffic("k_numeric_fp64", wl.name),
+                         "flops_per_launch": flops, "ms_per_launch": ms_num},
+            "roofline_hbm": {"bound": "hbm", "achieved": alg_bytes / (ms_tot * 1e-3) / 1e9,
+                             "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                             "frac": alg_bytes / (ms_tot * 1e-3) / 1e9 / peaks.get("hbm_gbs"),
+                             "note": f"algorithmic bytes of the whole multiply over its device time; {peak_kind}",
+                             "bytes": alg_bytes},
+            "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": statistics.mean(t_e2e) * 1e3},
+            "cpu_baseline": cpu,
+            "max_rel_err_vs_oracle": err,
+            "stats": {k: stats[-1][k] for k in ("n_products", "n_c_blocks", "ms_symbolic", "ms_numeric", "ms_total")},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    for m in (dc, db, da):
+        m.destroy()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,250 @@
+/*
+ * lamb_gpu.h -- C ABI of the B200 sector-based block-sparse multiply.
+ *
+ * This header is the drop-in boundary between a single-rank LAMB run and the
+ * GPU implementation of C = A . B over LAMB sector storage.  A Fortran caller
+ * binds it with ISO_C_BINDING (interface blocks are given in INTEGRATION.md);
+ * Python binds it with ctypes (lamb_b200/abi.py).
+ *
+ * Reference interfaces replaced (paths within uborstnik/LAMB):
+ *   - lamb_multiply(matrix_a, matrix_b, matrix_c, error)
+ *       src/lamb_multiplication.F90:116-204.  Its sector-pair loop (:180-201,
+ *       pair A(m,k) with B(k,n), C sector from lamb_plexus_get_sector_i) and
+ *       the sector_multiply stub (:206-225) are replaced by ONE call,
+ *       lamb_gpu_multiply(), over all sector triples.
+ *   - service_schedule / lamb_market_* / lamb_mp_window_* exchange
+ *       src/lamb_multiplication.F90:227-320, src/lamb_market_X_methods.F90:94-415:
+ *       at one rank every sector is local, so the exchange is a host no-op and
+ *       has no entry point here.
+ *   - Sector storage: lamb_sector_X_type (src/lamb_sector_X_types.F90:79-87),
+ *       lamb_index_type / lamb_blk_info_type (src/lamb_index_types.F90:86-105),
+ *       lamb_data_X_type (src/lamb_data_X_types.F90:77-83).  A sector crosses
+ *       the ABI as lamb_c_sector below; lamb_blk_info_type is not BIND(C), so
+ *       the caller repacks extents into one contiguous int64 array.
+ *
+ * Conventions (identical to the reference's sector storage):
+ *   row_p[n_rows+1]  int64, exclusive offsets, row_p[0] == 0, blocks of local
+ *                    row r are row_p[r] .. row_p[r+1]-1 (0-based block ids);
+ *                    src/lamb_index_methods.F90:248-274.
+ *   col_i[n_blks]    int16, 1-based local column, strictly increasing within
+ *                    a row (lamb_index_get_blk_n binary search,
+ *                    src/lamb_index_methods.F90:81-107, requires it).
+ *   extents[2*n_blks] int64 pairs (first,last), 1-based inclusive positions in
+ *                    data; last-first+1 == row_blk_size*col_blk_size.
+ *   data[data_len]   float64, each block column-major (Fortran order).
+ *   Block sizes are int8 (blksz_k, src/lamb_kinds.F90:175); zero is allowed.
+ *
+ * Status codes: every function returns int32.  0 is success.  A failure is
+ *   encoded as level*100000 + (type + 50000) where level is a LAMB error level
+ *   (src/lamb_error.F90:120-134: note 1 .. fatal 5) and type a LAMB error type
+ *   (src/lamb_error.F90:141-159, e.g. lamb_wrong_args = 100,
+ *   lamb_internal_error = -1, lamb_unimplemented = -1000,
+ *   lamb_external_error = -2000).  lamb_gpu_status_level/type decode it and
+ *   lamb_gpu_last_error() returns the message.  No exception, abort or exit
+ *   crosses this boundary.
+ *
+ * Threading: one context owns one CUDA stream and must be driven by one host
+ * thread at a time.  Calls are synchronous on return unless LAMB_GPU_ASYNC is
+ * given.
+ */
+#ifndef LAMB_GPU_H
+#define LAMB_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LAMB_API __attribute__((visibility("default")))
+#else
+#define LAMB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status encoding -------------------------------------------------- */
+#define LAMB_GPU_OK 0
+#define LAMB_LEVEL_NOTE 1
+#define LAMB_LEVEL_WARNING 2
+#define LAMB_LEVEL_FAILURE 3
+#define LAMB_LEVEL_MEMORY 4
+#define LAMB_LEVEL_FATAL 5
+#define LAMB_TYPE_CALLER_ERROR 1
+#define LAMB_TYPE_WRONG_ARGS 100
+#define LAMB_TYPE_PRECONDITION_FAILED 200
+#define LAMB_TYPE_INTERNAL_ERROR (-1)
+#define LAMB_TYPE_OVERFLOW_ERROR (-2)
+#define LAMB_TYPE_UNIMPLEMENTED (-1000)
+#define LAMB_TYPE_EXTERNAL_ERROR (-2000)
+
+/* ---- multiply flags ------------------------------------------------------ */
+#define LAMB_GPU_FP64 0u              /* plain FP64 block products            */
+#define LAMB_GPU_MIXED 1u             /* int8 split-slice products, FP64 recombination */
+#define LAMB_GPU_NO_PRODUCT_FILTER 2u /* keep products with |A_ik||B_kj| < eps */
+#define LAMB_GPU_NO_RESULT_FILTER 4u  /* keep C blocks with |C_ij| < eps      */
+#define LAMB_GPU_ASYNC 8u             /* return without synchronising         */
+#define LAMB_GPU_ACCUMULATE 16u       /* C := C + A.B on C's existing blocks (pattern of C is extended) */
+
+/* One sector of a LAMB matrix in the reference's storage (see above). */
+typedef struct lamb_c_sector {
+  int32_t subset_row;           /* subset position of the rows (1-based) */
+  int32_t subset_col;           /* subset position of the columns        */
+  int32_t n_rows;               /* atoms in the row subset               */
+  int32_t n_cols;               /* atoms in the column subset            */
+  const int8_t* row_blk_sizes;  /* [n_rows]                              */
+  const int8_t* col_blk_sizes;  /* [n_cols]                              */
+  const int64_t* row_p;         /* [n_rows+1]                            */
+  const int16_t* col_i;         /* [n_blks]                              */
+  const int64_t* extents;       /* [2*n_blks]                            */
+  const double* data;           /* [data_len]                            */
+  int64_t n_blks;
+  int64_t data_len;
+} lamb_c_sector;
+
+/* Writable sector for downloads; the caller allocates every array with the
+ * sizes returned by lamb_gpu_matrix_query (two-phase size->fill protocol,
+ * because the Fortran side owns its allocations:
+ * lamb_data_X_ensure_length / lamb_index_ensure_size). */
+typedef struct lamb_c_sector_out {
+  int32_t subset_row, subset_col, n_rows, n_cols;
+  int8_t* row_blk_sizes;
+  int8_t* col_blk_sizes;
+  int64_t* row_p;
+  int16_t* col_i;
+  int64_t* extents;
+  double* data;
+  int64_t n_blks;   /* in: capacity of col_i/extents; out: blocks written */
+  int64_t data_len; /* in: capacity of data; out: doubles written          */
+} lamb_c_sector_out;
+
+/* Sizes of one sector of a device matrix. */
+typedef struct lamb_c_sector_sizes {
+  int32_t subset_row, subset_col, n_rows, n_cols;
+  int64_t n_blks, data_len;
+} lamb_c_sector_sizes;
+
+/* Statistics of the last multiply on a context. */
+typedef struct lamb_gpu_mult_stats {
+  int64_t n_products;        /* block products executed (after the filter)   */
+  int64_t n_products_skipped;/* block products removed by the product filter */
+  int64_t n_c_blocks;        /* C blocks kept                                 */
+  int64_t n_c_blocks_dropped;/* C blocks removed by the result filter         */
+  double flops;              /* sum over executed products of 2*b_i*b_k*b_j   */
+  double ms_symbolic;        /* device time of the symbolic phase             */
+  double ms_numeric;         /* device time of the numeric phase              */
+  double ms_total;           /* device time of the whole multiply             */
+  int32_t mixed_slices;      /* int8 slices per operand (0 for FP64)          */
+  int32_t kernel_launches;   /* this library's kernels launched by the call   */
+} lamb_gpu_mult_stats;
+
+typedef struct lamb_gpu_ctx lamb_gpu_ctx;
+typedef int64_t lamb_gpu_matrix; /* handle, > 0 when valid */
+
+/* ---- context ------------------------------------------------------------- */
+/* Replaces nothing in the reference directly: it owns the CUDA stream and the
+ * device buffers that back lamb_data_X/lamb_index storage on the GPU
+ * (ownership mirrors lamb_data_X_type%mine, src/lamb_data_X_types.F90:80). */
+LAMB_API int32_t lamb_gpu_ctx_create(int32_t device, lamb_gpu_ctx** ctx);
+LAMB_API int32_t lamb_gpu_ctx_destroy(lamb_gpu_ctx* ctx);
+/* Copies the last error message (NUL-terminated, truncated to len). */
+LAMB_API int32_t lamb_gpu_last_error(const lamb_gpu_ctx* ctx, char* msg, int32_t len);
+LAMB_API int32_t lamb_gpu_status_level(int32_t status);
+LAMB_API int32_t lamb_gpu_status_type(int32_t status);
+/* Runs on the context's stream (cudaStream_t passed as void*). */
+LAMB_API int32_t lamb_gpu_ctx_get_stream(const lamb_gpu_ctx* ctx, void** stream);
+LAMB_API int32_t lamb_gpu_ctx_synchronize(lamb_gpu_ctx* ctx);
+
+/* ---- matrices -------------------------------------------------------------- */
+/* Uploads the local sectors of a matrix (lamb_matrix_X_type%sectors(:),
+ * src/lamb_matrix_X_types.F90:78-86) to device block-CSR storage.  Sectors
+ * may come in any order; each (subset_row, subset_col) at most once; a
+ * missing sector is empty.  Host arrays are not retained after return. */
+LAMB_API int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* ctx, const lamb_c_sector* sectors, int32_t n_sectors,
+                               lamb_gpu_matrix* handle);
+/* Creates an empty matrix with the row/column subsets of `like` (what
+ * lamb_matrix_copy + clearing gives the reference's C argument). */
+LAMB_API int32_t lamb_gpu_matrix_create_like(lamb_gpu_ctx* ctx, lamb_gpu_matrix like, lamb_gpu_matrix* handle);
+LAMB_API int32_t lamb_gpu_matrix_destroy(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle);
+/* Number of sectors, then per-sector sizes (sizes[n_sectors]). */
+LAMB_API int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, int32_t* n_sectors);
+LAMB_API int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_sizes* sizes,
+                              int32_t n_sectors);
+/* Fills caller-allocated sectors (out[n_sectors], order as from query). */
+LAMB_API int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_out* out,
+                                 int32_t n_sectors);
+
+/* ---- multiplication -------------------------------------------------------- */
+/* C := A . B (or C += A . B with LAMB_GPU_ACCUMULATE) over all sector triples
+ * (A(m,k), B(k,n)) -> C(m,n); replaces lamb_multiply
+ * (src/lamb_multiplication.F90:116-204).  A product A_ik.B_kj is skipped when
+ * |A_ik|_F*|B_kj|_F < eps and a C block is dropped when |C_ij|_F < eps
+ * (both switchable by flags; eps <= 0 disables both).  `c` must be a handle
+ * from lamb_gpu_matrix_create_like or a previous multiply; its contents are
+ * replaced.  stats may be NULL. */
+LAMB_API int32_t lamb_gpu_multiply(lamb_gpu_ctx* ctx, lamb_gpu_matrix a, lamb_gpu_matrix b, lamb_gpu_matrix c,
+                          double eps, uint32_t flags, lamb_gpu_mult_stats* stats);
+
+/* Symbolic phase only: builds C's pattern and the block-product stacks and
+ * exports the stacks in canonical order for checking.  Per C sector (order
+ * of lamb_gpu_matrix_query on the C handle after this call) the stack entries
+ * are int64 triples (a_sector, a_blk, b_sector, b_blk, c_blk) with 0-based
+ * sector indices into the A/B query order and 0-based block ids within the
+ * sector, grouped by block shape (m,n,k) = (row size of C, column size of C,
+ * inner size) in ascending order, and ordered by (C row, C column, k) within a
+ * group.  n_entries is the capacity on input and the count on output; with
+ * entries == NULL only the count is returned. */
+LAMB_API int32_t lamb_gpu_multiply_stacks(lamb_gpu_ctx* ctx, lamb_gpu_matrix a, lamb_gpu_matrix b, lamb_gpu_matrix c,
+                                 double eps, uint32_t flags, int64_t* entries, int64_t* n_entries);
+
+/* ---- block-sparse matrix algebra used by purification ------------------- */
+/* Y := alpha*X + beta*Y over the union pattern (result pattern of Y grows). */
+LAMB_API int32_t lamb_gpu_matrix_axpby(lamb_gpu_ctx* ctx, double alpha, lamb_gpu_matrix x, double beta, lamb_gpu_matrix y);
+/* Y := copy of X (pattern and values). */
+LAMB_API int32_t lamb_gpu_matrix_copy(lamb_gpu_ctx* ctx, lamb_gpu_matrix x, lamb_gpu_matrix y);
+/* trace(X) (diagonal blocks of diagonal sectors) and Tr(X.Y) = sum X_ij*Y_ji. */
+LAMB_API int32_t lamb_gpu_matrix_trace(lamb_gpu_ctx* ctx, lamb_gpu_matrix x, double* trace);
+LAMB_API int32_t lamb_gpu_matrix_trace_product(lamb_gpu_ctx* ctx, lamb_gpu_matrix x, lamb_gpu_matrix y, double* trace);
+/* |X|_F and |X - Y|_F over the union pattern. */
+LAMB_API int32_t lamb_gpu_matrix_frobenius(lamb_gpu_ctx* ctx, lamb_gpu_matrix x, double* norm);
+LAMB_API int32_t lamb_gpu_matrix_diff_frobenius(lamb_gpu_ctx* ctx, lamb_gpu_matrix x, lamb_gpu_matrix y, double* norm);
+/* X := alpha*X + shift*I (identity on the diagonal blocks). */
+LAMB_API int32_t lamb_gpu_matrix_scale_shift(lamb_gpu_ctx* ctx, lamb_gpu_matrix x, double alpha, double shift);
+
+/* ---- McWeeny purification ------------------------------------------------ */
+typedef struct lamb_gpu_purify_report {
+  int32_t steps_done;
+  int32_t steps_mixed;        /* steps whose products ran in the mixed mode  */
+  double trace;               /* Tr(P) after the last step                   */
+  double idempotency;         /* |P.P - P|_F / |P|_F after the last step     */
+  double ms_total;
+} lamb_gpu_purify_report;
+/* P_0 := (mu*I - H)*lambda/2 + I/2 with lambda from Gershgorin bounds of H,
+ * then `steps` iterations P := 3P^2 - 2P^3; the first steps-fp64_tail run with
+ * LAMB_GPU_MIXED products, the last fp64_tail in FP64.  p must come from
+ * lamb_gpu_matrix_create_like(h). */
+LAMB_API int32_t lamb_gpu_purify_mcweeny(lamb_gpu_ctx* ctx, lamb_gpu_matrix h, double mu, int32_t steps,
+                                int32_t fp64_tail, double eps, lamb_gpu_matrix p, lamb_gpu_purify_report* rep);
+
+/* ---- adjoint of C = A.B on a fixed pattern ------------------------------ */
+/* dA := (dC . B^T) restricted to A's pattern, dB := (A^T . dC) restricted to
+ * B's pattern.  dC must have C's pattern (any pattern is accepted: absent
+ * blocks count as zero).  dA/dB must come from create_like(a)/(b) and are
+ * overwritten with A's/B's pattern. */
+LAMB_API int32_t lamb_gpu_multiply_adjoint(lamb_gpu_ctx* ctx, lamb_gpu_matrix a, lamb_gpu_matrix b, lamb_gpu_matrix dc,
+                                  lamb_gpu_matrix da, lamb_gpu_matrix db);
+
+/* ---- batched multiplication ----------------------------------------------- */
+/* Many independent C_b = A_b . B_b (FP64) in one persistent launch over a
+ * global work queue, replayed from a captured CUDA graph.  All handles must
+ * be distinct matrices on this context; c[i] from create_like(a[i]). */
+typedef struct lamb_gpu_batch lamb_gpu_batch;
+LAMB_API int32_t lamb_gpu_batch_create(lamb_gpu_ctx* ctx, const lamb_gpu_matrix* a, const lamb_gpu_matrix* b,
+                              const lamb_gpu_matrix* c, int32_t n, double eps, lamb_gpu_batch** batch);
+/* Runs the batch once (first call captures the graph; later calls replay). */
+LAMB_API int32_t lamb_gpu_batch_execute(lamb_gpu_batch* batch, lamb_gpu_mult_stats* stats);
+LAMB_API int32_t lamb_gpu_batch_destroy(lamb_gpu_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LAMB_GPU_H */

@@ -1,0 +1,147 @@
+// Shared definitions of the B200 sector-multiply library (liblamb_b200.so).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lamb_gpu.h"
+
+namespace lamb {
+
+// ---- status codes (level/type pairs of src/lamb_error.F90:120-159) -------
+inline int32_t make_status(int level, int type) { return level * 100000 + (type + 50000); }
+
+// ---- device matrix ------------------------------------------------------------
+// Every device matrix is one block-CSR over "sector order": the atoms of
+// subset 1 first (in local order), then subset 2, ... along rows and columns.
+// A global row is a local row of one row subset; its blocks are sorted by
+// global column, so the blocks of sector (m,n) are a contiguous run of the row.
+// Block data live in one buffer, sector-major: all blocks of sector (m,n)
+// inside [sec_base[s], sec_base[s] + sec_dlen[s]), s = (m-1)*n_csub + (n-1).
+// Inside a sector the caller's layout (uploads) or CSR order (results) is kept.
+struct DevMatrix {
+  int32_t n_rsub = 0, n_csub = 0;
+  std::vector<int32_t> rsub_cnt, csub_cnt;    // atoms per subset
+  std::vector<int32_t> rsub_base, csub_base;  // first sector-order index of each subset (+ total)
+  std::vector<int8_t> h_row_bs, h_col_bs;     // block sizes (host copies)
+  int32_t n_rows = 0, n_cols = 0;
+  int64_t nnz = 0, data_len = 0;
+  std::vector<int64_t> sec_base, sec_dlen, sec_nblk;  // per sector (m,n)
+  int8_t* row_bs = nullptr;    // [n_rows]
+  int8_t* col_bs = nullptr;    // [n_cols]
+  int64_t* row_p = nullptr;    // [n_rows+1]
+  int32_t* col = nullptr;      // [nnz]
+  int64_t* off = nullptr;      // [nnz], 0-based data offset of each block
+  double* data = nullptr;      // [data_len]
+  double* norms = nullptr;     // [nnz] Frobenius norms, valid when norms_valid
+  bool norms_valid = false;
+  // For uploaded matrices: source sector and block id of every global block
+  // (used to express stacks in the caller's numbering).
+  int32_t* src_sec = nullptr;  // [nnz]
+  int64_t* src_blk = nullptr;  // [nnz]
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  std::map<int64_t, std::unique_ptr<DevMatrix>> mats;
+  int64_t next_handle = 1;
+  lamb_gpu_mult_stats last_stats{};
+  int64_t launches = 0;  // kernels of this library launched on the context
+  cudaEvent_t ev[8] = {};
+};
+
+// Error helpers: set the message, return the encoded status.
+int32_t fail(Ctx* ctx, int level, int type, const std::string& msg);
+#define LAMB_CUDA(ctx, call)                                                                             \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess)                                                                               \
+      return ::lamb::fail((ctx), LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR,                           \
+                          std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ":" +   \
+                              std::to_string(__LINE__) + ")");                                           \
+  } while (0)
+#define LAMB_TRY(x)                   \
+  do {                                \
+    int32_t st_ = (x);                \
+    if (st_ != LAMB_GPU_OK) return st_; \
+  } while (0)
+
+// Stream-ordered allocation on the context's stream.
+template <typename T>
+int32_t dalloc(Ctx* ctx, T** p, int64_t n) {
+  *p = nullptr;
+  if (n <= 0) return LAMB_GPU_OK;
+  cudaError_t e = cudaMallocAsync((void**)p, sizeof(T) * (size_t)n, ctx->stream);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(ctx, LAMB_LEVEL_MEMORY, LAMB_TYPE_EXTERNAL_ERROR,
+                std::string("device allocation of ") + std::to_string(sizeof(T) * (size_t)n) +
+                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  return LAMB_GPU_OK;
+}
+template <typename T>
+void dfree(Ctx* ctx, T*& p) {
+  if (p) cudaFreeAsync((void*)p, ctx->stream);
+  p = nullptr;
+}
+
+DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h);
+void free_matrix_buffers(Ctx* ctx, DevMatrix* m);
+int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h);
+int32_t ensure_norms(Ctx* ctx, DevMatrix* m);
+// Copies the subset structure (not the blocks) of rows of `r` and columns of `c`.
+void copy_structure(DevMatrix* dst, const DevMatrix* r_src, bool rows_from_rows, const DevMatrix* c_src,
+                    bool cols_from_cols);
+int32_t upload_block_sizes(Ctx* ctx, DevMatrix* m);
+// Sector-major layout for a pattern already in m (row_p/col set): fills off,
+// sec_base/sec_dlen/sec_nblk, data_len.  row_of (optional, [nnz]) gets each block's row.
+int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of);
+// Exclusive scan of int64 (in place allowed), via CUB with stream-ordered scratch.
+int32_t exclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
+int32_t inclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
+int32_t sum_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out);
+
+// ---- device helpers -------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// Fixed-order block norm: sequential fma over the block in storage order.
+// The CPU oracle uses the same expression, so the filter decisions agree bit for bit.
+__device__ __forceinline__ double block_norm_seq(const double* __restrict__ x, int64_t n) {
+  double s = 0.0;
+  for (int64_t e = 0; e < n; ++e) s = __fma_rn(x[e], x[e], s);
+  return __dsqrt_rn(s);
+}
+
+constexpr int kThreads = 256;
+// Counts a launch of one of this library's kernels and checks it.
+#define LAMB_LAUNCHED(ctx) do { ++(ctx)->launches; LAMB_CUDA((ctx), cudaGetLastError()); } while (0)
+inline int grid_for(int64_t n, int threads = kThreads, int cap = 148 * 64) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+}  // namespace lamb

@@ -1,0 +1,596 @@
+// Context, device matrices (upload / query / download / copy) and shared
+// device utilities of liblamb_b200.so.
+//
+// The device matrix replaces the reference's per-sector storage
+// (lamb_sector_X_type + lamb_index_type + lamb_data_X_type,
+// src/lamb_sector_X_types.F90:79-87, src/lamb_index_types.F90:86-105,
+// src/lamb_data_X_types.F90:77-83) with one block-CSR per matrix in sector
+// order; see DevMatrix in common.cuh.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace lamb {
+
+int32_t fail(Ctx* ctx, int level, int type, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return make_status(level, type);
+}
+
+DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h) {
+  auto it = ctx->mats.find(h);
+  return it == ctx->mats.end() ? nullptr : it->second.get();
+}
+
+void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
+  dfree(ctx, m->row_bs);
+  dfree(ctx, m->col_bs);
+  dfree(ctx, m->row_p);
+  dfree(ctx, m->col);
+  dfree(ctx, m->off);
+  dfree(ctx, m->data);
+  dfree(ctx, m->norms);
+  dfree(ctx, m->src_sec);
+  dfree(ctx, m->src_blk);
+  m->norms_valid = false;
+}
+
+int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h) {
+  *h = ctx->next_handle++;
+  ctx->mats[*h] = std::move(m);
+  return LAMB_GPU_OK;
+}
+
+void copy_structure(DevMatrix* d, const DevMatrix* r, bool rows_from_rows, const DevMatrix* c, bool cols_from_cols) {
+  if (rows_from_rows) {
+    d->n_rsub = r->n_rsub; d->rsub_cnt = r->rsub_cnt; d->rsub_base = r->rsub_base; d->h_row_bs = r->h_row_bs;
+    d->n_rows = r->n_rows;
+  } else {
+    d->n_rsub = r->n_csub; d->rsub_cnt = r->csub_cnt; d->rsub_base = r->csub_base; d->h_row_bs = r->h_col_bs;
+    d->n_rows = r->n_cols;
+  }
+  if (cols_from_cols) {
+    d->n_csub = c->n_csub; d->csub_cnt = c->csub_cnt; d->csub_base = c->csub_base; d->h_col_bs = c->h_col_bs;
+    d->n_cols = c->n_cols;
+  } else {
+    d->n_csub = c->n_rsub; d->csub_cnt = c->rsub_cnt; d->csub_base = c->rsub_base; d->h_col_bs = c->h_row_bs;
+    d->n_cols = c->n_rows;
+  }
+}
+
+int32_t upload_block_sizes(Ctx* ctx, DevMatrix* m) {
+  LAMB_TRY(dalloc(ctx, &m->row_bs, std::max(m->n_rows, 1)));
+  LAMB_TRY(dalloc(ctx, &m->col_bs, std::max(m->n_cols, 1)));
+  if (m->n_rows)
+    LAMB_CUDA(ctx, cudaMemcpyAsync(m->row_bs, m->h_row_bs.data(), m->n_rows, cudaMemcpyHostToDevice, ctx->stream));
+  if (m->n_cols)
+    LAMB_CUDA(ctx, cudaMemcpyAsync(m->col_bs, m->h_col_bs.data(), m->n_cols, cudaMemcpyHostToDevice, ctx->stream));
+  return LAMB_GPU_OK;
+}
+
+// ---- scans --------------------------------------------------------------------------
+int32_t exclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n) {
+  if (n <= 0) return LAMB_GPU_OK;
+  size_t bytes = 0;
+  LAMB_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, ctx->stream));
+  void* tmp = nullptr;
+  LAMB_TRY(dalloc(ctx, (char**)&tmp, (int64_t)bytes + 16));
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, ctx->stream);
+  cudaFreeAsync(tmp, ctx->stream);
+  LAMB_CUDA(ctx, e);
+  return LAMB_GPU_OK;
+}
+
+int32_t inclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n) {
+  if (n <= 0) return LAMB_GPU_OK;
+  size_t bytes = 0;
+  LAMB_CUDA(ctx, cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, n, ctx->stream));
+  void* tmp = nullptr;
+  LAMB_TRY(dalloc(ctx, (char**)&tmp, (int64_t)bytes + 16));
+  cudaError_t e = cub::DeviceScan::InclusiveSum(tmp, bytes, in, out, n, ctx->stream);
+  cudaFreeAsync(tmp, ctx->stream);
+  LAMB_CUDA(ctx, e);
+  return LAMB_GPU_OK;
+}
+
+int32_t sum_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out) {
+  *host_out = 0;
+  if (n <= 0) return LAMB_GPU_OK;
+  int64_t* d_out = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_out, 1));
+  size_t bytes = 0;
+  LAMB_CUDA(ctx, cub::DeviceReduce::Sum(nullptr, bytes, in, d_out, n, ctx->stream));
+  void* tmp = nullptr;
+  LAMB_TRY(dalloc(ctx, (char**)&tmp, (int64_t)bytes + 16));
+  cudaError_t e = cub::DeviceReduce::Sum(tmp, bytes, in, d_out, n, ctx->stream);
+  cudaFreeAsync(tmp, ctx->stream);
+  LAMB_CUDA(ctx, e);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_out);
+  return LAMB_GPU_OK;
+}
+
+// ---- block norms -----------------------------------------------------------------------
+// One warp per block row; each lane sums whole blocks sequentially (fixed order).
+__global__ void k_block_norms(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                              const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                              const int8_t* __restrict__ col_bs, const double* __restrict__ data,
+                              double* __restrict__ norms) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < n_rows; r += nwarps) {
+    const int bi = row_bs[r];
+    for (int64_t b = row_p[r] + lane; b < row_p[r + 1]; b += 32) {
+      const int64_t n = (int64_t)bi * col_bs[col[b]];
+      norms[b] = block_norm_seq(data + off[b], n);
+    }
+  }
+}
+
+int32_t ensure_norms(Ctx* ctx, DevMatrix* m) {
+  if (m->norms_valid) return LAMB_GPU_OK;
+  if (!m->norms) LAMB_TRY(dalloc(ctx, &m->norms, std::max<int64_t>(m->nnz, 1)));
+  if (m->nnz > 0) {
+    k_block_norms<<<grid_for((int64_t)m->n_rows * 32), kThreads, 0, ctx->stream>>>(
+        m->n_rows, m->row_p, m->col, m->off, m->row_bs, m->col_bs, m->data, m->norms);
+    LAMB_LAUNCHED(ctx);
+  }
+  m->norms_valid = true;
+  return LAMB_GPU_OK;
+}
+
+// ---- sector-major layout ------------------------------------------------------------
+// Part sizes: for row r (subset m, local l) and column subset n, the data
+// size and block count of the row's run in sector (m,n).  Stored at
+// idx(m,n,l) = rsub_base[m]*S + n*cnt[m] + l so that one exclusive scan over
+// the array gives sector-major offsets.
+__global__ void k_part_sizes(int32_t n_rows, int32_t n_rsub, int32_t S, const int32_t* __restrict__ rsub_base,
+                             const int32_t* __restrict__ csub_base, const int64_t* __restrict__ row_p,
+                             const int32_t* __restrict__ col, const int8_t* __restrict__ row_bs,
+                             const int8_t* __restrict__ col_bs, int64_t* __restrict__ dsz,
+                             int64_t* __restrict__ bcnt) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int m = 0;
+    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+    const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
+    const int64_t l = r - rsub_base[m];
+    const int64_t base = (int64_t)rsub_base[m] * S + l;
+    const int bi = row_bs[r];
+    int n = 0;
+    int64_t ds = 0, bc = 0;
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      const int c = col[b];
+      while (c >= csub_base[n + 1]) {
+        dsz[base + n * cnt] = ds;
+        bcnt[base + n * cnt] = bc;
+        ds = 0; bc = 0; ++n;
+      }
+      ds += (int64_t)bi * col_bs[c];
+      ++bc;
+    }
+    for (; n < S; ++n) {
+      dsz[base + n * cnt] = ds;
+      bcnt[base + n * cnt] = bc;
+      ds = 0; bc = 0;
+    }
+  }
+}
+
+__global__ void k_part_offsets(int32_t n_rows, int32_t n_rsub, int32_t S, const int32_t* __restrict__ rsub_base,
+                               const int32_t* __restrict__ csub_base, const int64_t* __restrict__ row_p,
+                               const int32_t* __restrict__ col, const int8_t* __restrict__ row_bs,
+                               const int8_t* __restrict__ col_bs, const int64_t* __restrict__ dbase,
+                               int64_t* __restrict__ off, int32_t* __restrict__ row_of) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int m = 0;
+    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+    const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
+    const int64_t l = r - rsub_base[m];
+    const int64_t base = (int64_t)rsub_base[m] * S + l;
+    const int bi = row_bs[r];
+    int n = 0;
+    int64_t o = dbase[base];
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      const int c = col[b];
+      while (c >= csub_base[n + 1]) { ++n; o = dbase[base + n * cnt]; }
+      off[b] = o;
+      o += (int64_t)bi * col_bs[c];
+      if (row_of) row_of[b] = (int32_t)r;
+    }
+  }
+}
+
+int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of) {
+  const int S = m->n_csub;
+  const int64_t n_seq = (int64_t)m->n_rows * S;
+  m->sec_base.assign((size_t)m->n_rsub * S, 0);
+  m->sec_dlen.assign((size_t)m->n_rsub * S, 0);
+  m->sec_nblk.assign((size_t)m->n_rsub * S, 0);
+  if (!m->off) LAMB_TRY(dalloc(ctx, &m->off, std::max<int64_t>(m->nnz, 1)));
+  if (n_seq == 0) { m->data_len = 0; return LAMB_GPU_OK; }
+  int32_t *d_rb = nullptr, *d_cb = nullptr;
+  int64_t *dsz = nullptr, *bcnt = nullptr, *dbase = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_rb, m->n_rsub + 1));
+  LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
+  LAMB_TRY(dalloc(ctx, &dsz, n_seq));
+  LAMB_TRY(dalloc(ctx, &bcnt, n_seq));
+  LAMB_TRY(dalloc(ctx, &dbase, n_seq));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
+  k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+                                                                    m->col, m->row_bs, m->col_bs, dsz, bcnt);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, dsz, dbase, n_seq));
+  k_part_offsets<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+                                                                      m->col, m->row_bs, m->col_bs, dbase, m->off,
+                                                                      row_of);
+  LAMB_LAUNCHED(ctx);
+  std::vector<int64_t> h_dsz(n_seq), h_bcnt(n_seq), h_dbase(n_seq);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(h_dsz.data(), dsz, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(h_bcnt.data(), bcnt, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(h_dbase.data(), dbase, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int a = 0; a < m->n_rsub; ++a)
+    for (int n = 0; n < S; ++n) {
+      const int64_t cnt = m->rsub_cnt[a];
+      const int64_t first = (int64_t)m->rsub_base[a] * S + n * cnt;
+      int64_t dl = 0, nb = 0;
+      for (int64_t l = 0; l < cnt; ++l) { dl += h_dsz[first + l]; nb += h_bcnt[first + l]; }
+      const size_t s = (size_t)a * S + n;
+      m->sec_base[s] = cnt ? h_dbase[first] : (s ? m->sec_base[s - 1] + m->sec_dlen[s - 1] : 0);
+      m->sec_dlen[s] = dl;
+      m->sec_nblk[s] = nb;
+    }
+  m->data_len = h_dbase[n_seq - 1] + h_dsz[n_seq - 1];
+  dfree(ctx, d_rb); dfree(ctx, d_cb); dfree(ctx, dsz); dfree(ctx, bcnt); dfree(ctx, dbase);
+  return LAMB_GPU_OK;
+}
+
+// ---- sector structure validation ------------------------------------------------
+static int32_t check_sector(Ctx* ctx, const lamb_c_sector& s, int idx) {
+  auto bad = [&](const std::string& w) {
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "sector " + std::to_string(idx) + ": " + w);
+  };
+  if (s.subset_row < 1 || s.subset_col < 1) return bad("subset positions must be >= 1");
+  if (s.n_rows < 0 || s.n_cols < 0 || s.n_blks < 0 || s.data_len < 0) return bad("negative size");
+  if (s.n_cols > 32767 || s.n_rows > 32767) return bad("more than 32767 atoms in a subset (int16 local index)");
+  if (!s.row_p) return bad("row_p is NULL");
+  if (s.n_rows && (!s.row_blk_sizes)) return bad("row_blk_sizes is NULL");
+  if (s.n_cols && (!s.col_blk_sizes)) return bad("col_blk_sizes is NULL");
+  if (s.n_blks && (!s.col_i || !s.extents)) return bad("col_i/extents is NULL");
+  if (s.data_len && !s.data) return bad("data is NULL");
+  if (s.row_p[0] != 0) return bad("row_p[0] must be 0");
+  if (s.row_p[s.n_rows] != s.n_blks) return bad("row_p[n_rows] must equal n_blks");
+  for (int32_t r = 0; r < s.n_rows; ++r) {
+    if (s.row_blk_sizes[r] < 0) return bad("negative block size");
+    if (s.row_p[r + 1] < s.row_p[r]) return bad("row_p must be non-decreasing");
+    int prev = 0;
+    for (int64_t b = s.row_p[r]; b < s.row_p[r + 1]; ++b) {
+      const int c = s.col_i[b];
+      if (c < 1 || c > s.n_cols) return bad("col_i out of range at block " + std::to_string(b));
+      if (c <= prev) return bad("col_i not strictly increasing in row " + std::to_string(r + 1));
+      prev = c;
+      const int64_t sz = (int64_t)s.row_blk_sizes[r] * s.col_blk_sizes[c - 1];
+      const int64_t f = s.extents[2 * b], l = s.extents[2 * b + 1];
+      if (l - f + 1 != sz) return bad("extent length does not match block size at block " + std::to_string(b));
+      if (sz > 0 && (f < 1 || l > s.data_len)) return bad("extent outside data at block " + std::to_string(b));
+    }
+  }
+  for (int32_t c = 0; c < s.n_cols; ++c)
+    if (s.col_blk_sizes[c] < 0) return bad("negative block size");
+  return LAMB_GPU_OK;
+}
+
+}  // namespace lamb
+
+using namespace lamb;
+
+// ============================== C ABI ========================================
+extern "C" {
+
+int32_t lamb_gpu_status_level(int32_t status) { return status == 0 ? 0 : status / 100000; }
+int32_t lamb_gpu_status_type(int32_t status) { return status == 0 ? 0 : status % 100000 - 50000; }
+
+int32_t lamb_gpu_ctx_create(int32_t device, lamb_gpu_ctx** out) {
+  if (!out) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
+  if (device < 0 || device >= n) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess || p.major < 10)
+    return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED);  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
+  auto* ctx = new Ctx;
+  ctx->device = device;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
+  }
+  for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  // Keep freed stream-ordered memory in the pool between calls.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  *out = reinterpret_cast<lamb_gpu_ctx*>(ctx);
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_ctx_destroy(lamb_gpu_ctx* c) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return LAMB_GPU_OK;
+  cudaSetDevice(ctx->device);
+  for (auto& kv : ctx->mats) free_matrix_buffers(ctx, kv.second.get());
+  ctx->mats.clear();
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_last_error(const lamb_gpu_ctx* c, char* msg, int32_t len) {
+  auto* ctx = reinterpret_cast<const Ctx*>(c);
+  if (!msg || len <= 0) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  const std::string& s = ctx ? ctx->last_error : std::string("no context");
+  size_t n = std::min<size_t>(s.size(), (size_t)len - 1);
+  memcpy(msg, s.data(), n);
+  msg[n] = 0;
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_ctx_get_stream(const lamb_gpu_ctx* c, void** stream) {
+  auto* ctx = reinterpret_cast<const Ctx*>(c);
+  if (!ctx || !stream) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  *stream = (void*)ctx->stream;
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_ctx_synchronize(lamb_gpu_ctx* c) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_t n_sec, lamb_gpu_matrix* handle) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  if (!handle || n_sec < 0 || (n_sec && !sec))
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "upload: bad arguments");
+  *handle = 0;
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < n_sec; ++i) LAMB_TRY(check_sector(ctx, sec[i], i));
+  auto m = std::make_unique<DevMatrix>();
+  for (int i = 0; i < n_sec; ++i) {
+    m->n_rsub = std::max(m->n_rsub, sec[i].subset_row);
+    m->n_csub = std::max(m->n_csub, sec[i].subset_col);
+  }
+  const int R = m->n_rsub, S = m->n_csub;
+  std::vector<int> sid((size_t)R * S, -1);
+  std::vector<const int8_t*> rbs(R, nullptr), cbs(S, nullptr);
+  m->rsub_cnt.assign(R, -1);
+  m->csub_cnt.assign(S, -1);
+  for (int i = 0; i < n_sec; ++i) {
+    const auto& s = sec[i];
+    const size_t k = (size_t)(s.subset_row - 1) * S + (s.subset_col - 1);
+    if (sid[k] >= 0) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "duplicate sector");
+    sid[k] = i;
+    int& rc = m->rsub_cnt[s.subset_row - 1];
+    if (rc < 0) { rc = s.n_rows; rbs[s.subset_row - 1] = s.row_blk_sizes; }
+    else if (rc != s.n_rows || memcmp(rbs[s.subset_row - 1], s.row_blk_sizes, s.n_rows))
+      return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "row subset sizes differ between sectors");
+    int& cc = m->csub_cnt[s.subset_col - 1];
+    if (cc < 0) { cc = s.n_cols; cbs[s.subset_col - 1] = s.col_blk_sizes; }
+    else if (cc != s.n_cols || memcmp(cbs[s.subset_col - 1], s.col_blk_sizes, s.n_cols))
+      return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "column subset sizes differ between sectors");
+  }
+  for (int a = 0; a < R; ++a)
+    if (m->rsub_cnt[a] < 0) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "a row subset has no sector");
+  for (int a = 0; a < S; ++a)
+    if (m->csub_cnt[a] < 0) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "a column subset has no sector");
+  m->rsub_base.assign(R + 1, 0);
+  m->csub_base.assign(S + 1, 0);
+  for (int a = 0; a < R; ++a) m->rsub_base[a + 1] = m->rsub_base[a] + m->rsub_cnt[a];
+  for (int a = 0; a < S; ++a) m->csub_base[a + 1] = m->csub_base[a] + m->csub_cnt[a];
+  m->n_rows = m->rsub_base[R];
+  m->n_cols = m->csub_base[S];
+  m->h_row_bs.resize(m->n_rows);
+  m->h_col_bs.resize(m->n_cols);
+  for (int a = 0; a < R; ++a) if (m->rsub_cnt[a]) memcpy(&m->h_row_bs[m->rsub_base[a]], rbs[a], m->rsub_cnt[a]);
+  for (int a = 0; a < S; ++a) if (m->csub_cnt[a]) memcpy(&m->h_col_bs[m->csub_base[a]], cbs[a], m->csub_cnt[a]);
+  // Global CSR (host), sector-major data.
+  m->sec_base.assign((size_t)R * S, 0);
+  m->sec_dlen.assign((size_t)R * S, 0);
+  m->sec_nblk.assign((size_t)R * S, 0);
+  int64_t dpos = 0, nnz = 0;
+  for (size_t k = 0; k < sid.size(); ++k) {
+    m->sec_base[k] = dpos;
+    if (sid[k] >= 0) {
+      m->sec_dlen[k] = sec[sid[k]].data_len;
+      m->sec_nblk[k] = sec[sid[k]].n_blks;
+      dpos += sec[sid[k]].data_len;
+      nnz += sec[sid[k]].n_blks;
+    }
+  }
+  m->data_len = dpos;
+  m->nnz = nnz;
+  std::vector<int64_t> h_row_p(m->n_rows + 1, 0), h_off(nnz);
+  std::vector<int32_t> h_col(nnz), h_src(nnz);
+  std::vector<int64_t> h_srcb(nnz);
+  int64_t p = 0;
+  for (int a = 0; a < R; ++a)
+    for (int l = 0; l < m->rsub_cnt[a]; ++l) {
+      for (int n = 0; n < S; ++n) {
+        const int i = sid[(size_t)a * S + n];
+        if (i < 0) continue;
+        const auto& s = sec[i];
+        for (int64_t b = s.row_p[l]; b < s.row_p[l + 1]; ++b) {
+          h_col[p] = m->csub_base[n] + s.col_i[b] - 1;
+          const int64_t sz = s.extents[2 * b + 1] - s.extents[2 * b] + 1;
+          h_off[p] = m->sec_base[(size_t)a * S + n] + (sz > 0 ? s.extents[2 * b] - 1 : 0);
+          h_src[p] = i;
+          h_srcb[p] = b;
+          ++p;
+        }
+      }
+      h_row_p[m->rsub_base[a] + l + 1] = p;
+    }
+  LAMB_TRY(upload_block_sizes(ctx, m.get()));
+  LAMB_TRY(dalloc(ctx, &m->row_p, m->n_rows + 1));
+  LAMB_TRY(dalloc(ctx, &m->col, std::max<int64_t>(nnz, 1)));
+  LAMB_TRY(dalloc(ctx, &m->off, std::max<int64_t>(nnz, 1)));
+  LAMB_TRY(dalloc(ctx, &m->src_sec, std::max<int64_t>(nnz, 1)));
+  LAMB_TRY(dalloc(ctx, &m->src_blk, std::max<int64_t>(nnz, 1)));
+  LAMB_TRY(dalloc(ctx, &m->data, std::max<int64_t>(m->data_len, 1)));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(m->row_p, h_row_p.data(), sizeof(int64_t) * (m->n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
+  if (nnz) {
+    LAMB_CUDA(ctx, cudaMemcpyAsync(m->col, h_col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(m->off, h_off.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(m->src_sec, h_src.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(m->src_blk, h_srcb.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  for (size_t k = 0; k < sid.size(); ++k)
+    if (sid[k] >= 0 && sec[sid[k]].data_len > 0)
+      LAMB_CUDA(ctx, cudaMemcpyAsync(m->data + m->sec_base[k], sec[sid[k]].data, sizeof(double) * sec[sid[k]].data_len,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+  // The host vectors above die at return: wait for the copies.
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return register_matrix(ctx, std::move(m), handle);
+}
+
+int32_t lamb_gpu_matrix_create_like(lamb_gpu_ctx* c, lamb_gpu_matrix like, lamb_gpu_matrix* handle) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx || !handle) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix* src = get_matrix(ctx, like);
+  if (!src) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "create_like: invalid handle");
+  cudaSetDevice(ctx->device);
+  auto m = std::make_unique<DevMatrix>();
+  copy_structure(m.get(), src, true, src, true);
+  LAMB_TRY(upload_block_sizes(ctx, m.get()));
+  LAMB_TRY(dalloc(ctx, &m->row_p, m->n_rows + 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(m->row_p, 0, sizeof(int64_t) * (m->n_rows + 1), ctx->stream));
+  m->sec_base.assign((size_t)m->n_rsub * m->n_csub, 0);
+  m->sec_dlen.assign((size_t)m->n_rsub * m->n_csub, 0);
+  m->sec_nblk.assign((size_t)m->n_rsub * m->n_csub, 0);
+  return register_matrix(ctx, std::move(m), handle);
+}
+
+int32_t lamb_gpu_matrix_destroy(lamb_gpu_ctx* c, lamb_gpu_matrix h) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  auto it = ctx->mats.find(h);
+  if (it == ctx->mats.end()) return fail(ctx, LAMB_LEVEL_WARNING, LAMB_TYPE_WRONG_ARGS, "destroy: invalid handle");
+  cudaSetDevice(ctx->device);
+  free_matrix_buffers(ctx, it->second.get());
+  ctx->mats.erase(it);
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* c, lamb_gpu_matrix h, int32_t* n) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx || !n) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix* m = get_matrix(ctx, h);
+  if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "invalid handle");
+  *n = m->n_rsub * m->n_csub;
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sector_sizes* sizes, int32_t n) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix* m = get_matrix(ctx, h);
+  if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "invalid handle");
+  if (!sizes || n != m->n_rsub * m->n_csub)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "query: sizes array must hold n_sectors entries");
+  for (int a = 0; a < m->n_rsub; ++a)
+    for (int b = 0; b < m->n_csub; ++b) {
+      auto& o = sizes[a * m->n_csub + b];
+      o.subset_row = a + 1;
+      o.subset_col = b + 1;
+      o.n_rows = m->rsub_cnt[a];
+      o.n_cols = m->csub_cnt[b];
+      o.n_blks = m->sec_nblk[(size_t)a * m->n_csub + b];
+      o.data_len = m->sec_dlen[(size_t)a * m->n_csub + b];
+    }
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sector_out* out, int32_t n) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix* m = get_matrix(ctx, h);
+  if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "invalid handle");
+  if (!out || n != m->n_rsub * m->n_csub)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: out array must hold n_sectors entries");
+  cudaSetDevice(ctx->device);
+  const int S = m->n_csub;
+  for (int a = 0; a < m->n_rsub; ++a)
+    for (int b = 0; b < S; ++b) {
+      auto& o = out[a * S + b];
+      const size_t s = (size_t)a * S + b;
+      if (o.n_blks < m->sec_nblk[s] || o.data_len < m->sec_dlen[s])
+        return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: capacity below queried size");
+      if ((m->sec_nblk[s] && (!o.col_i || !o.extents)) || (m->sec_dlen[s] && !o.data) || !o.row_p)
+        return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: NULL output array");
+    }
+  // Data first (largest copies), straight into the caller's arrays.
+  for (int a = 0; a < m->n_rsub; ++a)
+    for (int b = 0; b < S; ++b) {
+      const size_t s = (size_t)a * S + b;
+      if (m->sec_dlen[s])
+        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].data, m->data + m->sec_base[s], sizeof(double) * m->sec_dlen[s],
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  std::vector<int64_t> h_row_p(m->n_rows + 1), h_off(m->nnz);
+  std::vector<int32_t> h_col(m->nnz);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(h_row_p.data(), m->row_p, sizeof(int64_t) * (m->n_rows + 1), cudaMemcpyDeviceToHost, ctx->stream));
+  if (m->nnz) {
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_col.data(), m->col, sizeof(int32_t) * m->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_off.data(), m->off, sizeof(int64_t) * m->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int a = 0; a < m->n_rsub; ++a)
+    for (int b = 0; b < S; ++b) {
+      auto& o = out[a * S + b];
+      const size_t s = (size_t)a * S + b;
+      o.subset_row = a + 1;
+      o.subset_col = b + 1;
+      o.n_rows = m->rsub_cnt[a];
+      o.n_cols = m->csub_cnt[b];
+      if (o.row_blk_sizes && o.n_rows) memcpy(o.row_blk_sizes, &m->h_row_bs[m->rsub_base[a]], o.n_rows);
+      if (o.col_blk_sizes && o.n_cols) memcpy(o.col_blk_sizes, &m->h_col_bs[m->csub_base[b]], o.n_cols);
+      const int32_t c0 = m->csub_base[b], c1 = m->csub_base[b + 1];
+      int64_t q = 0;
+      o.row_p[0] = 0;
+      for (int l = 0; l < m->rsub_cnt[a]; ++l) {
+        const int r = m->rsub_base[a] + l;
+        const int bi = m->h_row_bs[r];
+        const int32_t* cb = h_col.data() + h_row_p[r];
+        const int32_t* ce = h_col.data() + h_row_p[r + 1];
+        const int32_t* lo = std::lower_bound(cb, ce, c0);
+        const int32_t* hi = std::lower_bound(lo, ce, c1);
+        for (const int32_t* it = lo; it != hi; ++it) {
+          const int64_t g = h_row_p[r] + (it - cb);
+          const int64_t sz = (int64_t)bi * m->h_col_bs[*it];
+          o.col_i[q] = (int16_t)(*it - c0 + 1);
+          o.extents[2 * q] = h_off[g] - m->sec_base[s] + 1;
+          o.extents[2 * q + 1] = h_off[g] - m->sec_base[s] + sz;
+          ++q;
+        }
+        o.row_p[l + 1] = q;
+      }
+      o.n_blks = q;
+      o.data_len = m->sec_dlen[s];
+    }
+  return LAMB_GPU_OK;
+}
+
+}  // extern "C"

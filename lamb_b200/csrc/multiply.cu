@@ -1,0 +1,715 @@
+// C = A.B over LAMB sectors on the GPU: symbolic phase, FP64 numeric phase,
+// result filter, and the lamb_gpu_multiply / lamb_gpu_multiply_stacks entry
+// points.
+//
+// Replaces lamb_multiply (src/lamb_multiplication.F90:116-204): its sector
+// pairing "A(m,k) with B(k',n) when k == k', into C(m,n)" (:180-201) is
+// realised by the sector-order block-CSR, in which A's column k and B's row k
+// index the same atom, so one global product visits exactly the sector
+// triples the reference pairs, with k subsets in ascending order.  The
+// sector_multiply stub (:206-225) becomes the numeric kernels below.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <numeric>
+
+#include "multiply.cuh"
+
+namespace lamb {
+
+void free_symbolic(Ctx* ctx, Symbolic& s) {
+  dfree(ctx, s.stack_p);
+  dfree(ctx, s.stack);
+  dfree(ctx, s.c_row);
+}
+
+int32_t check_compatible(Ctx* ctx, const DevMatrix* A, const DevMatrix* B) {
+  if (A->n_csub != B->n_rsub || A->csub_cnt != B->rsub_cnt || A->h_col_bs != B->h_row_bs)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS,
+                "A's column subsets and B's row subsets differ (A, B distributions do not match)");
+  return LAMB_GPU_OK;
+}
+
+// ---- symbolic phase ----------------------------------------------------------------
+// One CTA per C block row.  A bitmap over C's block columns marks the columns
+// reached by surviving products A_ik.B_kj (|A_ik|*|B_kj| >= eps).
+constexpr int kSymThreads = 256;
+
+__device__ __forceinline__ bool keep_pair(double na, double nb, double eps, int filt) {
+  return !(filt && na * nb < eps);
+}
+
+__global__ void __launch_bounds__(kSymThreads) k_sym_count(
+    int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
+    const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
+    const double* __restrict__ b_nrm, const int8_t* __restrict__ row_bs, const int8_t* __restrict__ k_bs,
+    const int8_t* __restrict__ col_bs, double eps, int filt, int32_t n_words, int64_t* __restrict__ c_cnt,
+    int64_t* __restrict__ s_cnt, int64_t* __restrict__ p_cnt, double* __restrict__ row_flops) {
+  extern __shared__ uint32_t bm[];
+  typedef cub::BlockReduce<int64_t, kSymThreads> RI;
+  typedef cub::BlockReduce<double, kSymThreads> RD;
+  __shared__ typename RI::TempStorage ti;
+  __shared__ typename RD::TempStorage td;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kSymThreads / 32;
+  for (int64_t i = blockIdx.x; i < n_rows; i += gridDim.x) {
+    for (int w = tid; w < n_words; w += kSymThreads) bm[w] = 0u;
+    __syncthreads();
+    int64_t kept = 0, pairs = 0;
+    double fl = 0.0;
+    const int bi = row_bs[i];
+    for (int64_t ab = a_row_p[i] + warp; ab < a_row_p[i + 1]; ab += nw) {
+      const int k = a_col[ab];
+      const double na = a_nrm[ab];
+      const int bk = k_bs[k];
+      const int64_t b1 = b_row_p[k + 1];
+      for (int64_t bb = b_row_p[k] + lane; bb < b1; bb += 32) {
+        ++pairs;
+        if (!keep_pair(na, b_nrm[bb], eps, filt)) continue;
+        const int j = b_col[bb];
+        atomicOr(&bm[j >> 5], 1u << (j & 31));
+        ++kept;
+        fl += 2.0 * bi * bk * col_bs[j];
+      }
+    }
+    __syncthreads();
+    int64_t pc = 0;
+    for (int w = tid; w < n_words; w += kSymThreads) pc += __popc(bm[w]);
+    int64_t tot_pc = RI(ti).Sum(pc);
+    __syncthreads();
+    int64_t tot_kept = RI(ti).Sum(kept);
+    __syncthreads();
+    int64_t tot_pairs = RI(ti).Sum(pairs);
+    __syncthreads();
+    double tot_fl = RD(td).Sum(fl);
+    if (tid == 0) {
+      c_cnt[i] = tot_pc;
+      s_cnt[i] = tot_kept;
+      p_cnt[i] = tot_pairs;
+      row_flops[i] = tot_fl;
+    }
+    __syncthreads();
+  }
+}
+
+// Exclusive block scan of v[0..n) in place; returns the total.
+__device__ int block_excl_scan_smem(int* v, int n) {
+  typedef cub::BlockScan<int, kSymThreads> BS;
+  __shared__ typename BS::TempStorage ts;
+  __shared__ int total;
+  const int tid = threadIdx.x;
+  const int per = (n + kSymThreads - 1) / kSymThreads;
+  const int lo = min(n, tid * per), hi = min(n, lo + per);
+  int s = 0;
+  for (int t = lo; t < hi; ++t) s += v[t];
+  int ex, agg;
+  BS(ts).ExclusiveSum(s, ex, agg);
+  __syncthreads();
+  for (int t = lo; t < hi; ++t) {
+    const int x = v[t];
+    v[t] = ex;
+    ex += x;
+  }
+  if (tid == 0) total = agg;
+  __syncthreads();
+  return total;
+}
+
+__device__ __forceinline__ int bm_rank(const uint32_t* bm, const int* wpre, int j) {
+  return wpre[j >> 5] + __popc(bm[j >> 5] & ((1u << (j & 31)) - 1u));
+}
+
+__global__ void __launch_bounds__(kSymThreads) k_sym_fill(
+    int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
+    const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
+    const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, const int64_t* __restrict__ c_row_p,
+    const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col, int64_t* __restrict__ stack_p,
+    int2* __restrict__ stack) {
+  extern __shared__ uint32_t sm[];
+  uint32_t* bm = sm;
+  int* wpre = (int*)(sm + n_words);
+  int* cur = wpre + n_words;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kSymThreads / 32;
+  for (int64_t i = blockIdx.x; i < n_rows; i += gridDim.x) {
+    for (int w = tid; w < n_words; w += kSymThreads) bm[w] = 0u;
+    __syncthreads();
+    const int64_t a0 = a_row_p[i], a1 = a_row_p[i + 1];
+    for (int64_t ab = a0 + warp; ab < a1; ab += nw) {
+      const int k = a_col[ab];
+      const double na = a_nrm[ab];
+      for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
+        if (keep_pair(na, b_nrm[bb], eps, filt)) {
+          const int j = b_col[bb];
+          atomicOr(&bm[j >> 5], 1u << (j & 31));
+        }
+    }
+    __syncthreads();
+    for (int w = tid; w < n_words; w += kSymThreads) wpre[w] = __popc(bm[w]);
+    __syncthreads();
+    block_excl_scan_smem(wpre, n_words);
+    const int64_t c0 = c_row_p[i];
+    const int nc = (int)(c_row_p[i + 1] - c0);
+    // C columns of the row, ascending.
+    for (int w = tid; w < n_words; w += kSymThreads) {
+      uint32_t bits = bm[w];
+      int p = wpre[w];
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        c_col[c0 + p++] = w * 32 + b;
+      }
+    }
+    for (int t = tid; t < nc; t += kSymThreads) cur[t] = 0;
+    __syncthreads();
+    for (int64_t ab = a0 + warp; ab < a1; ab += nw) {
+      const int k = a_col[ab];
+      const double na = a_nrm[ab];
+      for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
+        if (keep_pair(na, b_nrm[bb], eps, filt)) atomicAdd(&cur[bm_rank(bm, wpre, b_col[bb])], 1);
+    }
+    __syncthreads();
+    block_excl_scan_smem(cur, nc);
+    const int64_t sb = s_row_base[i];
+    for (int t = tid; t < nc; t += kSymThreads) stack_p[c0 + t] = sb + cur[t];
+    __syncthreads();
+    // Entries in k order: one A block at a time; the B row's columns are
+    // distinct, so each C position advances at most once per A block.
+    for (int64_t ab = a0; ab < a1; ++ab) {
+      const int k = a_col[ab];
+      const double na = a_nrm[ab];
+      for (int64_t bb = b_row_p[k] + tid; bb < b_row_p[k + 1]; bb += kSymThreads)
+        if (keep_pair(na, b_nrm[bb], eps, filt)) {
+          const int p = bm_rank(bm, wpre, b_col[bb]);
+          const int slot = cur[p];
+          cur[p] = slot + 1;
+          stack[sb + slot] = make_int2((int)ab, (int)bb);
+        }
+      __syncthreads();
+    }
+  }
+}
+
+int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, Symbolic* out) {
+  *out = Symbolic{};
+  LAMB_TRY(check_compatible(ctx, A, B));
+  LAMB_TRY(ensure_norms(ctx, A));
+  LAMB_TRY(ensure_norms(ctx, B));
+  if (A->nnz >= (1ll << 31) || B->nnz >= (1ll << 31))
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "more than 2^31 blocks in an operand");
+  // C takes A's row subsets and B's column subsets.
+  free_matrix_buffers(ctx, C);
+  copy_structure(C, A, true, B, true);
+  LAMB_TRY(upload_block_sizes(ctx, C));
+  const int32_t n_rows = C->n_rows;
+  const int32_t n_words = (C->n_cols + 31) / 32;
+  LAMB_TRY(dalloc(ctx, &C->row_p, n_rows + 1));
+  int64_t *c_cnt = nullptr, *s_cnt = nullptr, *p_cnt = nullptr;
+  double* rfl = nullptr;
+  LAMB_TRY(dalloc(ctx, &c_cnt, std::max(n_rows, 1)));
+  LAMB_TRY(dalloc(ctx, &s_cnt, std::max(n_rows, 1)));
+  LAMB_TRY(dalloc(ctx, &p_cnt, std::max(n_rows, 1)));
+  LAMB_TRY(dalloc(ctx, &rfl, std::max(n_rows, 1)));
+  const int fl = filt ? 1 : 0;
+  const size_t smem_count = sizeof(uint32_t) * (size_t)std::max(n_words, 1);
+  if (smem_count > 200 * 1024)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "too many block columns for the symbolic bitmap");
+  const int grid = std::max(1, std::min(n_rows, 148 * 8));
+  if (n_rows > 0) {
+    if (smem_count > 48 * 1024)
+      LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count));
+    k_sym_count<<<grid, kSymThreads, smem_count, ctx->stream>>>(
+        n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, C->row_bs, B->row_bs, C->col_bs, eps, fl,
+        n_words, c_cnt, s_cnt, p_cnt, rfl);
+    LAMB_LAUNCHED(ctx);
+  }
+  std::vector<int64_t> h_c(n_rows), h_s(n_rows), h_p(n_rows);
+  std::vector<double> h_f(n_rows);
+  if (n_rows) {
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_c.data(), c_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_s.data(), s_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_p.data(), p_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_f.data(), rfl, sizeof(double) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  std::vector<int64_t> h_crp(n_rows + 1, 0), h_srb(n_rows + 1, 0);
+  int64_t max_c = 0;
+  for (int r = 0; r < n_rows; ++r) {
+    h_crp[r + 1] = h_crp[r] + h_c[r];
+    h_srb[r + 1] = h_srb[r] + h_s[r];
+    out->n_pairs += h_p[r];
+    out->flops += h_f[r];
+    max_c = std::max(max_c, h_c[r]);
+  }
+  out->c_nnz = h_crp[n_rows];
+  out->n_ent = h_srb[n_rows];
+  if (out->n_ent >= (1ll << 40))
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "stack too large");
+  C->nnz = out->c_nnz;
+  int64_t* s_row_base = nullptr;
+  LAMB_TRY(dalloc(ctx, &s_row_base, n_rows + 1));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(C->row_p, h_crp.data(), sizeof(int64_t) * (n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(s_row_base, h_srb.data(), sizeof(int64_t) * (n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_TRY(dalloc(ctx, &C->col, std::max<int64_t>(C->nnz, 1)));
+  LAMB_TRY(dalloc(ctx, &out->stack_p, C->nnz + 1));
+  LAMB_TRY(dalloc(ctx, &out->stack, std::max<int64_t>(out->n_ent, 1)));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+  const size_t smem_fill = sizeof(uint32_t) * (size_t)std::max(n_words, 1) * 2 + sizeof(int) * (size_t)(max_c + 1);
+  if (smem_fill > 220 * 1024)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
+  if (n_rows > 0 && C->nnz > 0) {
+    if (smem_fill > 48 * 1024)
+      LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
+    k_sym_fill<<<grid, kSymThreads, smem_fill, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col,
+                                                               B->norms, eps, fl, n_words, C->row_p, s_row_base,
+                                                               C->col, out->stack_p, out->stack);
+    LAMB_LAUNCHED(ctx);
+  }
+  LAMB_TRY(dalloc(ctx, &out->c_row, std::max<int64_t>(C->nnz, 1)));
+  LAMB_TRY(layout_sector_major(ctx, C, out->c_row));
+  LAMB_TRY(dalloc(ctx, &C->data, std::max<int64_t>(C->data_len, 1)));
+  dfree(ctx, c_cnt); dfree(ctx, s_cnt); dfree(ctx, p_cnt); dfree(ctx, rfl); dfree(ctx, s_row_base);
+  return LAMB_GPU_OK;
+}
+
+// ---- A meta: data offset and k block size in one word -----------------------------
+__global__ void k_pack_a_meta(int64_t nnz, const int32_t* __restrict__ col, const int64_t* __restrict__ off,
+                              const int8_t* __restrict__ col_bs, int64_t* __restrict__ out) {
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nnz; b += (int64_t)gridDim.x * blockDim.x)
+    out[b] = off[b] | ((int64_t)col_bs[col[b]] << 56);
+}
+
+int32_t pack_a_meta(Ctx* ctx, const DevMatrix* A, int64_t** a_offk) {
+  LAMB_TRY(dalloc(ctx, a_offk, std::max<int64_t>(A->nnz, 1)));
+  if (A->data_len > kOffMask) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "A data too large");
+  if (A->nnz) {
+    k_pack_a_meta<<<grid_for(A->nnz), kThreads, 0, ctx->stream>>>(A->nnz, A->col, A->off, A->col_bs, *a_offk);
+    LAMB_LAUNCHED(ctx);
+  }
+  return LAMB_GPU_OK;
+}
+
+// ---- FP64 numeric phase ---------------------------------------------------------------
+// One warp owns one C block (segment ownership: no atomics).  The block's
+// stack is consumed as one concatenated K dimension: sum_e A_ik(e) . B_k(e)j
+// = [A_ik1 | A_ik2 | ...] . [B_k1j; B_k2j; ...], padded to a multiple of 4
+// once per 32 entries instead of once per entry.  Products run on the FP64
+// tensor pipe with mma.m8n8k4 (DMMA): MF x NF fragments of 8x8 cover the
+// b_i x b_j block.  Fragment layouts (PTX ISA, mma.m8n8k4 .f64):
+//   A (8x4, row): lane holds A[lane/4][lane%4]
+//   B (4x8, col): lane holds B[lane%4][lane/4]
+//   C (8x8):      lane holds C[lane/4][2*(lane%4) + {0,1}]
+constexpr int kNumWarps = 8;
+
+struct WarpMeta {
+  long long ao[32];
+  long long bo[32];
+  int pre[33];
+};
+
+__device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int MF, int NF>
+__device__ __forceinline__ void cblock_fp64(const double* __restrict__ Ad, const double* __restrict__ Bd,
+                                            double* __restrict__ Cd, int bi, int bj, int64_t c_off, int64_t s0,
+                                            int64_t s1, const int2* __restrict__ stk,
+                                            const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off,
+                                            WarpMeta& wm, double* __restrict__ c_nrm, int64_t c) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[MF][NF][2];
+#pragma unroll
+  for (int i = 0; i < MF; ++i)
+#pragma unroll
+    for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int64_t base = s0; base < s1; base += 32) {
+    const int n = (int)min((int64_t)32, s1 - base);
+    int bk = 0;
+    long long ao = 0, bo = 0;
+    if (lane < n) {
+      const int2 e = stk[base + lane];
+      const long long ak = a_offk[e.x];
+      ao = ak & kOffMask;
+      bk = (int)(ak >> 56);
+      bo = b_off[e.y];
+    }
+    const int incl = warp_incl_scan(bk, lane);
+    wm.ao[lane] = ao;
+    wm.bo[lane] = bo;
+    wm.pre[lane] = incl - bk;
+    if (lane == 31) wm.pre[32] = incl;
+    __syncwarp();
+    const int K = wm.pre[32];
+    int e = 0;
+    for (int kw = 0; kw < K; kw += 4) {
+      const int colk = kw + t;
+      while (e < n - 1 && colk >= wm.pre[e + 1]) ++e;
+      const bool valid = colk < K;
+      const int kc = colk - wm.pre[e];
+      const int bke = wm.pre[e + 1] - wm.pre[e];
+      const double* pa = Ad + wm.ao[e] + (int64_t)kc * bi;
+      const double* pb = Bd + wm.bo[e] + kc;
+      double av[MF], bv[NF];
+#pragma unroll
+      for (int i = 0; i < MF; ++i) {
+        const int r = i * 8 + g;
+        av[i] = (valid && r < bi) ? __ldg(pa + r) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < NF; ++j) {
+        const int cc = j * 8 + g;
+        bv[j] = (valid && cc < bj) ? __ldg(pb + (int64_t)cc * bke) : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < MF; ++i)
+#pragma unroll
+        for (int j = 0; j < NF; ++j) dmma884(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
+    }
+    __syncwarp();
+  }
+  double sq = 0.0;
+#pragma unroll
+  for (int i = 0; i < MF; ++i)
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = i * 8 + g, cc = j * 8 + 2 * t + h;
+        if (r < bi && cc < bj) {
+          const double v = acc[i][j][h];
+          Cd[c_off + (int64_t)cc * bi + r] = v;
+          sq = __fma_rn(v, v, sq);
+        }
+      }
+  sq = warp_sum(sq);
+  if (lane == 0 && c_nrm) c_nrm[c] = __dsqrt_rn(sq);
+}
+
+// Generic path for blocks wider than 24 rows or columns: plain FP64 FMAs,
+// one C element per lane and step.
+__device__ void cblock_fp64_generic(const double* __restrict__ Ad, const double* __restrict__ Bd,
+                                    double* __restrict__ Cd, int bi, int bj, int64_t c_off, int64_t s0, int64_t s1,
+                                    const int2* __restrict__ stk, const int64_t* __restrict__ a_offk,
+                                    const int64_t* __restrict__ b_off, double* __restrict__ c_nrm, int64_t c) {
+  const int lane = threadIdx.x & 31;
+  double sq = 0.0;
+  for (int el = lane; el < bi * bj; el += 32) {
+    const int r = el % bi, cc = el / bi;
+    double acc = 0.0;
+    for (int64_t s = s0; s < s1; ++s) {
+      const int2 e = stk[s];
+      const long long ak = a_offk[e.x];
+      const int bk = (int)(ak >> 56);
+      const double* pa = Ad + (ak & kOffMask);
+      const double* pb = Bd + b_off[e.y];
+      for (int kk = 0; kk < bk; ++kk) acc = __fma_rn(pa[(int64_t)kk * bi + r], pb[(int64_t)cc * bk + kk], acc);
+    }
+    Cd[c_off + (int64_t)cc * bi + r] = acc;
+    sq = __fma_rn(acc, acc, sq);
+  }
+  sq = warp_sum(sq);
+  if (lane == 0 && c_nrm) c_nrm[c] = __dsqrt_rn(sq);
+}
+
+__global__ void __launch_bounds__(kNumWarps * 32) k_numeric_fp64(
+    int64_t c_nnz, const int32_t* __restrict__ c_row, const int32_t* __restrict__ c_col,
+    const int64_t* __restrict__ c_off, const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs,
+    const int64_t* __restrict__ stack_p, const int2* __restrict__ stk, const int64_t* __restrict__ a_offk,
+    const int64_t* __restrict__ b_off, const double* __restrict__ Ad, const double* __restrict__ Bd,
+    double* __restrict__ Cd, double* __restrict__ c_nrm) {
+  __shared__ WarpMeta wms[kNumWarps];
+  const int w = threadIdx.x >> 5;
+  WarpMeta& wm = wms[w];
+  const int64_t nwarps = (int64_t)gridDim.x * kNumWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kNumWarps + w; c < c_nnz; c += nwarps) {
+    const int bi = row_bs[c_row[c]], bj = col_bs[c_col[c]];
+    const int64_t co = c_off[c], s0 = stack_p[c], s1 = stack_p[c + 1];
+    const int mf = (bi + 7) >> 3, nf = (bj + 7) >> 3;
+    switch (mf * 4 + nf) {
+      case 0 * 4 + 0: case 0 * 4 + 1: case 0 * 4 + 2: case 0 * 4 + 3: case 1 * 4 + 0: case 2 * 4 + 0:
+      case 3 * 4 + 0:  // a zero-size block: no data, norm 0
+        if ((threadIdx.x & 31) == 0 && c_nrm) c_nrm[c] = 0.0;
+        break;
+      case 1 * 4 + 1: cblock_fp64<1, 1>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 1 * 4 + 2: cblock_fp64<1, 2>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 1 * 4 + 3: cblock_fp64<1, 3>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 2 * 4 + 1: cblock_fp64<2, 1>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 2 * 4 + 2: cblock_fp64<2, 2>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 2 * 4 + 3: cblock_fp64<2, 3>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 3 * 4 + 1: cblock_fp64<3, 1>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 3 * 4 + 2: cblock_fp64<3, 2>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      case 3 * 4 + 3: cblock_fp64<3, 3>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
+      default: cblock_fp64_generic(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, c_nrm, c); break;
+    }
+  }
+}
+
+int32_t numeric_fp64(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, DevMatrix* C, const Symbolic& sym,
+                     const int64_t* a_offk, double* c_nrm) {
+  if (sym.c_nnz == 0) return LAMB_GPU_OK;
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  int per_sm = 0;
+  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_numeric_fp64, kNumWarps * 32, 0));
+  const int64_t need = (sym.c_nnz + kNumWarps - 1) / kNumWarps;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)dev_sms * std::max(per_sm, 1)));
+  k_numeric_fp64<<<grid, kNumWarps * 32, 0, ctx->stream>>>(sym.c_nnz, sym.c_row, C->col, C->off, C->row_bs,
+                                                            C->col_bs, sym.stack_p, sym.stack, a_offk, B->off,
+                                                            A->data, B->data, C->data, c_nrm);
+  LAMB_LAUNCHED(ctx);
+  return LAMB_GPU_OK;
+}
+
+// ---- result filter ----------------------------------------------------------------------
+// Keeps C block c iff !(c_nrm[c] < eps).  Counts per (row, column subset)
+// give the new row pointers and per-sector block counts; the data stay where
+// they are (extents may leave holes in a sector's data, as LAMB's data
+// stores allow).
+__global__ void k_keep_counts(int32_t n_rows, int32_t S, const int32_t* __restrict__ csub_base,
+                              const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                              const double* __restrict__ c_nrm, double eps, int64_t* __restrict__ keep_rn) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int n = 0;
+    int64_t k = 0;
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      while (col[b] >= csub_base[n + 1]) { keep_rn[r * S + n] = k; k = 0; ++n; }
+      k += !(c_nrm[b] < eps);
+    }
+    for (; n < S; ++n) { keep_rn[r * S + n] = k; k = 0; }
+  }
+}
+
+__global__ void k_compact(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                          const int64_t* __restrict__ off, const double* __restrict__ c_nrm, double eps,
+                          const int64_t* __restrict__ new_row_p, int32_t* __restrict__ ncol,
+                          int64_t* __restrict__ noff) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int64_t q = new_row_p[r];
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b)
+      if (!(c_nrm[b] < eps)) { ncol[q] = col[b]; noff[q] = off[b]; ++q; }
+  }
+}
+
+int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps, int64_t* dropped) {
+  *dropped = 0;
+  const int S = C->n_csub;
+  const int64_t n = (int64_t)C->n_rows * S;
+  if (C->nnz == 0 || n == 0) return LAMB_GPU_OK;
+  int64_t* keep_rn = nullptr;
+  int32_t* d_cb = nullptr;
+  LAMB_TRY(dalloc(ctx, &keep_rn, n));
+  LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, C->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
+  k_keep_counts<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, S, d_cb, C->row_p, C->col, c_nrm, eps, keep_rn);
+  LAMB_LAUNCHED(ctx);
+  std::vector<int64_t> h(n);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(h.data(), keep_rn, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::vector<int64_t> nrp(C->n_rows + 1, 0);
+  std::vector<int64_t> snb((size_t)C->n_rsub * S, 0);
+  int a = 0;
+  for (int r = 0; r < C->n_rows; ++r) {
+    while (a + 1 < C->n_rsub && C->rsub_base[a + 1] <= r) ++a;
+    int64_t k = 0;
+    for (int c = 0; c < S; ++c) { k += h[(int64_t)r * S + c]; snb[(size_t)a * S + c] += h[(int64_t)r * S + c]; }
+    nrp[r + 1] = nrp[r] + k;
+  }
+  const int64_t kept = nrp[C->n_rows];
+  *dropped = C->nnz - kept;
+  if (*dropped == 0) { dfree(ctx, keep_rn); dfree(ctx, d_cb); return LAMB_GPU_OK; }
+  int64_t* d_nrp = nullptr;
+  int32_t* ncol = nullptr;
+  int64_t* noff = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_nrp, C->n_rows + 1));
+  LAMB_TRY(dalloc(ctx, &ncol, std::max<int64_t>(kept, 1)));
+  LAMB_TRY(dalloc(ctx, &noff, std::max<int64_t>(kept, 1)));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_nrp, nrp.data(), sizeof(int64_t) * (C->n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
+  k_compact<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, C->off, c_nrm, eps, d_nrp, ncol, noff);
+  LAMB_LAUNCHED(ctx);
+  dfree(ctx, C->row_p); dfree(ctx, C->col); dfree(ctx, C->off);
+  C->row_p = d_nrp; C->col = ncol; C->off = noff;
+  C->nnz = kept;
+  C->sec_nblk = snb;
+  C->norms_valid = false;
+  dfree(ctx, keep_rn); dfree(ctx, d_cb);
+  return LAMB_GPU_OK;
+}
+
+// ---- driver -------------------------------------------------------------------------------
+int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, uint32_t flags,
+                      lamb_gpu_mult_stats* stats) {
+  if (A == C || B == C)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "C must be distinct from A and B");
+  if (flags & LAMB_GPU_ACCUMULATE)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "LAMB_GPU_ACCUMULATE: use lamb_gpu_matrix_axpby");
+  const bool filt_p = eps > 0 && !(flags & LAMB_GPU_NO_PRODUCT_FILTER);
+  const bool filt_r = eps > 0 && !(flags & LAMB_GPU_NO_RESULT_FILTER);
+  const bool timed = !(flags & LAMB_GPU_ASYNC);
+  lamb_gpu_mult_stats st{};
+  const int64_t launches0 = ctx->launches;
+  if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+  Symbolic sym;
+  int32_t rc = symbolic_phase(ctx, A, B, C, eps, filt_p, &sym);
+  if (rc != LAMB_GPU_OK) { free_symbolic(ctx, sym); return rc; }
+  if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+  int64_t* a_offk = nullptr;
+  double* c_nrm = nullptr;
+  rc = pack_a_meta(ctx, A, &a_offk);
+  if (rc == LAMB_GPU_OK) rc = dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1));
+  if (rc == LAMB_GPU_OK && timed) rc = cudaEventRecord(ctx->ev[2], ctx->stream) == cudaSuccess ? 0 : rc;
+  int slices = 0;
+  if (rc == LAMB_GPU_OK) {
+    if (flags & LAMB_GPU_MIXED)
+      rc = numeric_mixed(ctx, A, B, C, sym, a_offk, c_nrm, &slices);
+    else
+      rc = numeric_fp64(ctx, A, B, C, sym, a_offk, c_nrm);
+  }
+  if (rc == LAMB_GPU_OK && timed) rc = cudaEventRecord(ctx->ev[3], ctx->stream) == cudaSuccess ? 0 : rc;
+  int64_t dropped = 0;
+  if (rc == LAMB_GPU_OK && filt_r) rc = result_filter(ctx, C, c_nrm, eps, &dropped);
+  if (rc == LAMB_GPU_OK && timed) rc = cudaEventRecord(ctx->ev[4], ctx->stream) == cudaSuccess ? 0 : rc;
+  dfree(ctx, a_offk);
+  dfree(ctx, c_nrm);
+  free_symbolic(ctx, sym);
+  if (rc != LAMB_GPU_OK) return rc;
+  C->norms_valid = false;
+  st.n_products = sym.n_ent;
+  st.n_products_skipped = sym.n_pairs - sym.n_ent;
+  st.n_c_blocks = C->nnz;
+  st.n_c_blocks_dropped = dropped;
+  st.flops = sym.flops;
+  st.mixed_slices = slices;
+  st.kernel_launches = (int32_t)(ctx->launches - launches0);
+  if (timed) {
+    LAMB_CUDA(ctx, cudaEventSynchronize(ctx->ev[4]));
+    float t01 = 0, t23 = 0, t04 = 0;
+    cudaEventElapsedTime(&t01, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&t23, ctx->ev[2], ctx->ev[3]);
+    cudaEventElapsedTime(&t04, ctx->ev[0], ctx->ev[4]);
+    st.ms_symbolic = t01;
+    st.ms_numeric = t23;
+    st.ms_total = t04;
+  }
+  ctx->last_stats = st;
+  if (stats) *stats = st;
+  return LAMB_GPU_OK;
+}
+
+// ---- stacks in the caller's numbering ----------------------------------------------------
+// Sector and sector-local block id of every block of a device matrix, from its CSR.
+static void host_block_ids(const DevMatrix* m, const std::vector<int64_t>& row_p, const std::vector<int32_t>& col,
+                           std::vector<int32_t>& sec, std::vector<int64_t>& lid) {
+  const int S = m->n_csub;
+  sec.assign(col.size(), 0);
+  lid.assign(col.size(), 0);
+  std::vector<int64_t> cnt((size_t)m->n_rsub * S, 0);
+  for (int a = 0; a < m->n_rsub; ++a)
+    for (int l = 0; l < m->rsub_cnt[a]; ++l) {
+      const int r = m->rsub_base[a] + l;
+      int n = 0;
+      for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+        while (col[b] >= m->csub_base[n + 1]) ++n;
+        const size_t s = (size_t)a * S + n;
+        sec[b] = (int32_t)s;
+        lid[b] = cnt[s]++;
+      }
+    }
+}
+
+static int32_t stacks_export(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym,
+                             int64_t* entries, int64_t* n_entries) {
+  auto d2h_csr = [&](const DevMatrix* m, std::vector<int64_t>& rp, std::vector<int32_t>& cl) -> int32_t {
+    rp.resize(m->n_rows + 1);
+    cl.resize(m->nnz);
+    LAMB_CUDA(ctx, cudaMemcpyAsync(rp.data(), m->row_p, sizeof(int64_t) * (m->n_rows + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    if (m->nnz)
+      LAMB_CUDA(ctx, cudaMemcpyAsync(cl.data(), m->col, sizeof(int32_t) * m->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    return LAMB_GPU_OK;
+  };
+  std::vector<int64_t> arp, brp, crp, sp(sym.c_nnz + 1);
+  std::vector<int32_t> acl, bcl, ccl;
+  std::vector<int2> st(sym.n_ent);
+  LAMB_TRY(d2h_csr(A, arp, acl));
+  LAMB_TRY(d2h_csr(B, brp, bcl));
+  LAMB_TRY(d2h_csr(C, crp, ccl));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(sp.data(), sym.stack_p, sizeof(int64_t) * (sym.c_nnz + 1), cudaMemcpyDeviceToHost, ctx->stream));
+  if (sym.n_ent)
+    LAMB_CUDA(ctx, cudaMemcpyAsync(st.data(), sym.stack, sizeof(int2) * sym.n_ent, cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!entries) { *n_entries = sym.n_ent; return LAMB_GPU_OK; }
+  if (*n_entries < sym.n_ent) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "stacks: capacity too small");
+  std::vector<int32_t> asec, bsec, csec;
+  std::vector<int64_t> alid, blid, clid;
+  host_block_ids(A, arp, acl, asec, alid);
+  host_block_ids(B, brp, bcl, bsec, blid);
+  host_block_ids(C, crp, ccl, csec, clid);
+  // C blocks of every sector in sector CSR order.
+  const int S = C->n_csub;
+  std::vector<std::vector<int64_t>> by_sec((size_t)C->n_rsub * S);
+  for (int r = 0; r < C->n_rows; ++r)
+    for (int64_t b = crp[r]; b < crp[r + 1]; ++b) by_sec[csec[b]].push_back(b);
+  int64_t out = 0;
+  struct E { int bi, bj, bk; int64_t seq; int64_t v[5]; };
+  std::vector<E> v;
+  for (size_t s = 0; s < by_sec.size(); ++s) {
+    v.clear();
+    int64_t seq = 0;
+    for (int64_t cb : by_sec[s]) {
+      int r = (int)(std::upper_bound(crp.begin(), crp.end(), cb) - crp.begin() - 1);
+      const int bi = C->h_row_bs[r], bj = C->h_col_bs[ccl[cb]];
+      for (int64_t e = sp[cb]; e < sp[cb + 1]; ++e) {
+        const int ab = st[e].x, bb = st[e].y;
+        const int bk = A->h_col_bs[acl[ab]];
+        v.push_back(E{bi, bj, bk, seq++, {asec[ab], alid[ab], bsec[bb], blid[bb], clid[cb]}});
+      }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const E& x, const E& y) {
+      if (x.bi != y.bi) return x.bi < y.bi;
+      if (x.bj != y.bj) return x.bj < y.bj;
+      return x.bk < y.bk;
+    });
+    for (const E& e : v) {
+      for (int f = 0; f < 5; ++f) entries[5 * out + f] = e.v[f];
+      ++out;
+    }
+  }
+  *n_entries = out;
+  return LAMB_GPU_OK;
+}
+
+}  // namespace lamb
+
+using namespace lamb;
+
+extern "C" {
+
+int32_t lamb_gpu_multiply(lamb_gpu_ctx* c, lamb_gpu_matrix a, lamb_gpu_matrix b, lamb_gpu_matrix cm, double eps,
+                          uint32_t flags, lamb_gpu_mult_stats* stats) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix *A = get_matrix(ctx, a), *B = get_matrix(ctx, b), *C = get_matrix(ctx, cm);
+  if (!A || !B || !C) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "multiply: invalid handle");
+  if (eps != eps) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "multiply: eps is NaN");
+  cudaSetDevice(ctx->device);
+  return multiply_impl(ctx, A, B, C, eps, flags, stats);
+}
+
+int32_t lamb_gpu_multiply_stacks(lamb_gpu_ctx* c, lamb_gpu_matrix a, lamb_gpu_matrix b, lamb_gpu_matrix cm,
+                                 double eps, uint32_t flags, int64_t* entries, int64_t* n_entries) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx || !n_entries) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix *A = get_matrix(ctx, a), *B = get_matrix(ctx, b), *C = get_matrix(ctx, cm);
+  if (!A || !B || !C || A == C || B == C)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "stacks: invalid handle");
+  cudaSetDevice(ctx->device);
+  const bool filt_p = eps > 0 && !(flags & LAMB_GPU_NO_PRODUCT_FILTER);
+  Symbolic sym;
+  int32_t rc = symbolic_phase(ctx, A, B, C, eps, filt_p, &sym);
+  if (rc == LAMB_GPU_OK) rc = stacks_export(ctx, A, B, C, sym, entries, n_entries);
+  free_symbolic(ctx, sym);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,259 @@
+"""Python host side of the C ABI (include/lamb_gpu.h), mirroring LAMB's
+multiplication interface.
+
+``lamb_multiply(matrix_a, matrix_b, matrix_c)`` keeps the argument meaning of
+``lamb_multiply(matrix_a, matrix_b, matrix_c, error)``
+(src/lamb_multiplication.F90:116-119): A and B are read, C is replaced by
+A.B.  Errors surface as ``LambError`` carrying the LAMB error level and type
+(src/lamb_error.F90:120-159) decoded from the C status.
+
+There is no CPU fallback: every call goes through liblamb_b200.so and fails
+loudly when the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .abi import CSector, CSectorOut, CSectorSizes, MultStats, PurifyReport, sector_to_c
+from .matrix import LambMatrix, Sector
+
+FP64 = 0
+MIXED = 1
+NO_PRODUCT_FILTER = 2
+NO_RESULT_FILTER = 4
+ASYNC = 8
+
+LEVELS = {1: "note", 2: "warning", 3: "failure", 4: "memory", 5: "fatal"}
+TYPES = {1: "caller_error", 100: "wrong_args", 200: "precondition_failed", -1: "internal_error",
+         -2: "overflow_error", -100: "invariant_failed", -200: "postcondition_failed", -300: "assertion_failed",
+         -1000: "unimplemented", -2000: "external_error"}
+
+
+class LambError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        self.status = status
+        self.level = status // 100000 if status else 0
+        self.type = status % 100000 - 50000 if status else 0
+        super().__init__(f"[{LEVELS.get(self.level, self.level)}/{TYPES.get(self.type, self.type)}] {msg}")
+
+
+_typed = False
+
+
+def lib() -> C.CDLL:
+    global _typed
+    L = _lib.load("liblamb_b200.so")
+    if not _typed:
+        vp, i32, i64, dbl, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_uint32
+        P = C.POINTER
+        sig = {
+            "lamb_gpu_ctx_create": [i32, P(vp)],
+            "lamb_gpu_ctx_destroy": [vp],
+            "lamb_gpu_last_error": [vp, C.c_char_p, i32],
+            "lamb_gpu_status_level": [i32],
+            "lamb_gpu_status_type": [i32],
+            "lamb_gpu_ctx_get_stream": [vp, P(vp)],
+            "lamb_gpu_ctx_synchronize": [vp],
+            "lamb_gpu_matrix_upload": [vp, P(CSector), i32, P(i64)],
+            "lamb_gpu_matrix_create_like": [vp, i64, P(i64)],
+            "lamb_gpu_matrix_destroy": [vp, i64],
+            "lamb_gpu_matrix_n_sectors": [vp, i64, P(i32)],
+            "lamb_gpu_matrix_query": [vp, i64, P(CSectorSizes), i32],
+            "lamb_gpu_matrix_download": [vp, i64, P(CSectorOut), i32],
+            "lamb_gpu_multiply": [vp, i64, i64, i64, dbl, u32, P(MultStats)],
+            "lamb_gpu_multiply_stacks": [vp, i64, i64, i64, dbl, u32, vp, P(i64)],
+            "lamb_gpu_matrix_axpby": [vp, dbl, i64, dbl, i64],
+            "lamb_gpu_matrix_copy": [vp, i64, i64],
+            "lamb_gpu_matrix_trace": [vp, i64, P(dbl)],
+            "lamb_gpu_matrix_trace_product": [vp, i64, i64, P(dbl)],
+            "lamb_gpu_matrix_frobenius": [vp, i64, P(dbl)],
+            "lamb_gpu_matrix_diff_frobenius": [vp, i64, i64, P(dbl)],
+            "lamb_gpu_matrix_scale_shift": [vp, i64, dbl, dbl],
+            "lamb_gpu_purify_mcweeny": [vp, i64, dbl, i32, i32, dbl, i64, P(PurifyReport)],
+            "lamb_gpu_multiply_adjoint": [vp, i64, i64, i64, i64, i64],
+            "lamb_gpu_batch_create": [vp, P(i64), P(i64), P(i64), i32, dbl, P(vp)],
+            "lamb_gpu_batch_execute": [vp, P(MultStats)],
+            "lamb_gpu_batch_destroy": [vp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.argtypes = args
+            f.restype = i32
+        _typed = True
+    return L
+
+
+class Context:
+    """One CUDA device and stream (lamb_gpu_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        st = lib().lamb_gpu_ctx_create(device, C.byref(self._h))
+        if st != 0:
+            raise LambError(st, f"cannot create a context on device {device} (needs an sm_100 GPU)")
+        self.device = device
+
+    def check(self, st: int) -> None:
+        if st != 0:
+            buf = C.create_string_buffer(1024)
+            lib().lamb_gpu_last_error(self._h, buf, 1024)
+            raise LambError(st, buf.value.decode(errors="replace"))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        self.check(lib().lamb_gpu_ctx_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def synchronize(self) -> None:
+        self.check(lib().lamb_gpu_ctx_synchronize(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().lamb_gpu_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- matrices ---------------------------------------------------------------
+    def upload(self, m: LambMatrix) -> "DeviceMatrix":
+        arr = (CSector * len(m.sectors))(*[sector_to_c(s) for s in m.sectors])
+        h = C.c_int64()
+        self.check(lib().lamb_gpu_matrix_upload(self._h, arr, len(m.sectors), C.byref(h)))
+        return DeviceMatrix(self, h.value)
+
+    def create_like(self, like: "DeviceMatrix") -> "DeviceMatrix":
+        h = C.c_int64()
+        self.check(lib().lamb_gpu_matrix_create_like(self._h, like.h, C.byref(h)))
+        return DeviceMatrix(self, h.value)
+
+    def multiply(self, a: "DeviceMatrix", b: "DeviceMatrix", c: "DeviceMatrix", eps: float = 0.0,
+                 flags: int = 0) -> dict:
+        st = MultStats()
+        self.check(lib().lamb_gpu_multiply(self._h, a.h, b.h, c.h, eps, flags, C.byref(st)))
+        return st.as_dict()
+
+    def stacks(self, a: "DeviceMatrix", b: "DeviceMatrix", c: "DeviceMatrix", eps: float = 0.0,
+               flags: int = 0) -> np.ndarray:
+        n = C.c_int64(0)
+        self.check(lib().lamb_gpu_multiply_stacks(self._h, a.h, b.h, c.h, eps, flags, None, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 5), np.int64)
+        self.check(lib().lamb_gpu_multiply_stacks(self._h, a.h, b.h, c.h, eps, flags, out.ctypes.data, C.byref(n)))
+        return out[:n.value]
+
+
+class DeviceMatrix:
+    """A matrix resident on the GPU (lamb_gpu_matrix handle)."""
+
+    def __init__(self, ctx: Context, h: int):
+        self.ctx, self.h = ctx, h
+
+    def sizes(self) -> List[CSectorSizes]:
+        n = C.c_int32()
+        self.ctx.check(lib().lamb_gpu_matrix_n_sectors(self.ctx.handle, self.h, C.byref(n)))
+        arr = (CSectorSizes * n.value)()
+        self.ctx.check(lib().lamb_gpu_matrix_query(self.ctx.handle, self.h, arr, n.value))
+        return list(arr)
+
+    def download(self, pinned: bool = False, out: Optional[LambMatrix] = None) -> LambMatrix:
+        """Two-phase download: query sizes, allocate (or reuse `out`'s arrays
+        when they are large enough), fill.  Returned arrays are views trimmed
+        to the downloaded sizes."""
+        sz = self.sizes()
+        secs, outs = [], []
+        for i, s in enumerate(sz):
+            alloc = _pinned_empty if pinned else np.empty
+            old = out.sectors[i] if out is not None and i < len(out.sectors) else None
+
+            def take(a, n, dt, shape=None):
+                if a is not None and a.dtype == dt and a.size >= n and a.flags.c_contiguous:
+                    v = a.reshape(-1)[:n]
+                else:
+                    v = (alloc if dt == np.float64 else np.empty)(n, dt)
+                return v.reshape(shape) if shape else v
+
+            sec = Sector(s.subset_row, s.subset_col,
+                         take(old.row_blk_sizes if old else None, s.n_rows, np.int8),
+                         take(old.col_blk_sizes if old else None, s.n_cols, np.int8),
+                         take(old.row_p if old else None, s.n_rows + 1, np.int64),
+                         take(old.col_i if old else None, s.n_blks, np.int16),
+                         take(old.extents if old else None, 2 * s.n_blks, np.int64, (s.n_blks, 2)),
+                         take(old.data if old else None, s.data_len, np.float64))
+            secs.append(sec)
+            o = CSectorOut(s.subset_row, s.subset_col, s.n_rows, s.n_cols,
+                           _p(sec.row_blk_sizes), _p(sec.col_blk_sizes), _p(sec.row_p), _p(sec.col_i),
+                           _p(sec.extents), _p(sec.data), s.n_blks, s.data_len)
+            outs.append(o)
+        arr = (CSectorOut * len(outs))(*outs)
+        self.ctx.check(lib().lamb_gpu_matrix_download(self.ctx.handle, self.h, arr, len(outs)))
+        return LambMatrix(secs, "C")
+
+    def destroy(self) -> None:
+        if self.h:
+            lib().lamb_gpu_matrix_destroy(self.ctx.handle, self.h)
+            self.h = 0
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data if a.size else 0
+
+
+_pinned_keep = []
+
+
+def _pinned_empty(n: int, dtype) -> np.ndarray:
+    import torch
+    t = torch.empty(int(n) * np.dtype(dtype).itemsize, dtype=torch.uint8, pin_memory=True)
+    a = t.numpy().view(dtype)
+    _pinned_keep.append(t)
+    if len(_pinned_keep) > 64:
+        del _pinned_keep[:-64]
+    return a
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def lamb_multiply(matrix_a: LambMatrix, matrix_b: LambMatrix, matrix_c: Optional[LambMatrix] = None,
+                  eps: float = 0.0, flags: int = FP64, ctx: Optional[Context] = None, stats: Optional[dict] = None
+                  ) -> LambMatrix:
+    """C := A.B on the GPU through the C ABI; returns C (also stored into
+    matrix_c's sector list when given, like the reference's intent(inout))."""
+    ctx = ctx or default_context()
+    da = ctx.upload(matrix_a)
+    db = da if matrix_b is matrix_a else ctx.upload(matrix_b)
+    dc = ctx.create_like(da)
+    try:
+        st = ctx.multiply(da, db, dc, eps, flags)
+        if stats is not None:
+            stats.update(st)
+        c = dc.download()
+    finally:
+        dc.destroy()
+        if db is not da:
+            db.destroy()
+        da.destroy()
+    if matrix_c is not None:
+        matrix_c.sectors = c.sectors
+        return matrix_c
+    return c

@@ -1,0 +1,181 @@
+"""GPU multiply against the CPU oracle, through the C ABI (liblamb_b200.so).
+
+Bar: C block pattern and stacks bit-exact, values within 1e-12 relative
+Frobenius error of the oracle (FP64 path)."""
+import numpy as np
+import pytest
+
+import oracle
+from lamb_b200 import gpu
+from lamb_b200.gen import WATER_192, WATER_6144, WaterGeometry, random_fill_matrix
+from lamb_b200.matrix import LambMatrix, Sector
+from tests.helpers import assert_same_pattern, block_values, rel_frobenius_error
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+
+
+def _gpu_mult(ctx, a, b, eps, flags=0):
+    da = ctx.upload(a)
+    db = da if b is a else ctx.upload(b)
+    dc = ctx.create_like(da)
+    st = ctx.multiply(da, db, dc, eps, flags)
+    c = dc.download()
+    stk = None
+    for m in (dc, db, da):
+        m.destroy()
+    return c, st
+
+
+def _no_borderline(c_ref, eps):
+    if eps <= 0:
+        return
+    for v in block_values(c_ref).values():
+        n = float(np.sqrt(np.sum(v ** 2)))
+        assert abs(n - eps) > 1e-9 * eps, "a C block norm sits on the filter threshold"
+
+
+def _with_values(a, seed):
+    rng = np.random.default_rng(seed)
+    return LambMatrix([Sector(s.subset_row, s.subset_col, s.row_blk_sizes, s.col_blk_sizes, s.row_p, s.col_i,
+                              s.extents, rng.random(s.data.shape[0])) for s in a.sectors])
+
+
+def test_water192_cut6_parity(gpu_ctx):
+    g, a, b = WATER_192.build()
+    c_ref, st_ref = oracle.multiply(a, b, WATER_192.eps)
+    _no_borderline(c_ref, WATER_192.eps)
+    c, st = _gpu_mult(gpu_ctx, a, b, WATER_192.eps)
+    c.validate()
+    assert_same_pattern(c, c_ref)
+    assert rel_frobenius_error(c, c_ref) <= TOL_FP64
+    assert st["n_products"] == st_ref["n_products"]
+    assert st["n_products_skipped"] == st_ref["n_products_skipped"]
+    assert st["flops"] == st_ref["flops"]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 4, 7])
+def test_random_fill_parity(gpu_ctx, seed):
+    a = random_fill_matrix(seed)
+    b = _with_values(a, seed + 50)
+    c_ref, st_ref = oracle.multiply(a, b, 0.0)
+    c, st = _gpu_mult(gpu_ctx, a, b, 0.0)
+    assert_same_pattern(c, c_ref)
+    assert rel_frobenius_error(c, c_ref) <= TOL_FP64
+
+
+def test_empty_and_tiny(gpu_ctx):
+    a = random_fill_matrix(0, n_atoms=0)
+    c, st = _gpu_mult(gpu_ctx, a, a, 0.0)
+    assert all(s.n_blks == 0 for s in c.sectors)
+    a = random_fill_matrix(3, n_atoms=1)
+    c_ref, _ = oracle.multiply(a, a, 0.0)
+    c, _ = _gpu_mult(gpu_ctx, a, a, 0.0)
+    assert_same_pattern(c, c_ref)
+
+
+@pytest.mark.parametrize("seed", [0, 5])
+def test_stacks_bit_exact(gpu_ctx, seed):
+    g = WaterGeometry(48, None, 6.0, seed=seed)
+    a, b = g.matrix(seed + 1), g.matrix(seed + 2)
+    _, _, stk_ref = oracle.multiply(a, b, 0.0, want_stacks=True)
+    da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+    dc = gpu_ctx.create_like(da)
+    stk = gpu_ctx.stacks(da, db, dc, 0.0)
+    assert np.array_equal(stk, stk_ref)
+    for m in (dc, db, da):
+        m.destroy()
+
+
+def test_stacks_random_fill_zero_size_blocks(gpu_ctx):
+    a = random_fill_matrix(9)
+    b = _with_values(a, 3)
+    _, _, stk_ref = oracle.multiply(a, b, 0.0, want_stacks=True)
+    da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+    dc = gpu_ctx.create_like(da)
+    assert np.array_equal(gpu_ctx.stacks(da, db, dc, 0.0), stk_ref)
+
+
+def test_product_filter_parity(gpu_ctx):
+    g = WaterGeometry(64, None, 7.0, seed=8)
+    a, b = g.matrix(3), g.matrix(4)
+    # eps near the middle of the product-norm distribution: many products drop
+    eps = 2e-3
+    c_ref, st_ref, stk_ref = oracle.multiply(a, b, eps, oracle.NO_RESULT_FILTER, want_stacks=True)
+    assert st_ref["n_products_skipped"] > 0
+    c, st = _gpu_mult(gpu_ctx, a, b, eps, gpu.NO_RESULT_FILTER)
+    assert st["n_products_skipped"] == st_ref["n_products_skipped"]
+    assert_same_pattern(c, c_ref)
+    assert rel_frobenius_error(c, c_ref) <= TOL_FP64
+    da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+    dc = gpu_ctx.create_like(da)
+    assert np.array_equal(gpu_ctx.stacks(da, db, dc, eps, gpu.NO_RESULT_FILTER), stk_ref)
+
+
+def test_result_filter_parity(gpu_ctx):
+    g = WaterGeometry(64, None, 7.0, seed=8)
+    a, b = g.matrix(5), g.matrix(6)
+    eps = 0.3
+    c_ref, st_ref = oracle.multiply(a, b, eps, oracle.NO_PRODUCT_FILTER)
+    assert st_ref["n_c_blocks_dropped"] > 0
+    _no_borderline(c_ref, eps)
+    c, st = _gpu_mult(gpu_ctx, a, b, eps, gpu.NO_PRODUCT_FILTER)
+    assert st["n_c_blocks_dropped"] == st_ref["n_c_blocks_dropped"]
+    assert_same_pattern(c, c_ref)
+    assert rel_frobenius_error(c, c_ref) <= TOL_FP64
+
+
+def test_python_lamb_multiply_api(gpu_ctx):
+    g = WaterGeometry(32, None, 6.0, seed=1)
+    a = g.matrix(1)
+    c_ref, _ = oracle.multiply(a, a, 1e-8)
+    holder = LambMatrix([], "C")
+    out = gpu.lamb_multiply(a, a, holder, eps=1e-8, ctx=gpu_ctx)
+    assert out is holder
+    assert rel_frobenius_error(holder, c_ref) <= TOL_FP64
+
+
+def test_errors_are_reported_not_raised_through_abi(gpu_ctx):
+    a = WaterGeometry(16, None, 5.0, seed=1).matrix(1)
+    b = WaterGeometry(20, None, 5.0, seed=2).matrix(1)
+    da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+    dc = gpu_ctx.create_like(da)
+    with pytest.raises(gpu.LambError) as ei:
+        gpu_ctx.multiply(da, db, dc, 0.0)
+    assert ei.value.type == 100 and ei.value.level == 3
+    with pytest.raises(gpu.LambError):
+        gpu_ctx.multiply(da, da, da, 0.0)  # C aliases A
+    bad = WaterGeometry(16, None, 5.0, seed=1).matrix(1)
+    bad.sectors[0].col_i[0] = 32000
+    with pytest.raises(gpu.LambError) as ei:
+        gpu_ctx.upload(bad)
+    assert ei.value.type == 100
+
+
+def _rows_of(m: LambMatrix, stride: int):
+    out = {}
+    for s in m.sectors:
+        rows = s.block_rows()
+        for b in range(s.n_blks):
+            r = int(rows[b])
+            if r % stride == 0:
+                c = int(s.col_i[b]) - 1
+                f, l = int(s.extents[b, 0]), int(s.extents[b, 1])
+                out[(s.subset_row, s.subset_col, r, c)] = s.data[f - 1:l]
+    return out
+
+
+def test_water6144_cut8_sampled_rows(gpu_ctx):
+    """Full-size workload: GPU C against the oracle on every 61st row."""
+    g, a, b = WATER_6144.build()
+    c, st = _gpu_mult(gpu_ctx, a, b, WATER_6144.eps)
+    c.validate()
+    stride = 61
+    c_ref, st_ref = oracle.multiply(a, b, WATER_6144.eps, row_stride=stride)
+    got, ref = _rows_of(c, stride), _rows_of(c_ref, stride)
+    assert set(got) == set(ref)
+    num = sum(float(np.sum((got[k] - ref[k]) ** 2)) for k in ref)
+    den = sum(float(np.sum(ref[k] ** 2)) for k in ref)
+    assert np.sqrt(num / den) <= TOL_FP64
+    assert st["n_c_blocks"] == sum(s.n_blks for s in c.sectors)
