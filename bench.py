@@ -44,16 +44,17 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="water6144_cut8", choices=["water6144_cut8", "water192_cut6"])
+    p.add_argument("--workload", default="water6144_cut8", choices=["water6144_cut8", "water1536_cut7", "water192_cut6"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--no-positions", action="store_true", help="order work from the block pattern only")
     return p.parse_args()
 
 
 def workload(name):
     from lamb_b200 import gen
-    return {"water6144_cut8": gen.WATER_6144, "water192_cut6": gen.WATER_192}[name]
+    return {"water6144_cut8": gen.WATER_6144, "water1536_cut7": gen.WATER_1536, "water192_cut6": gen.WATER_192}[name]
 
 
 def algorithmic_bytes(a, b, c) -> int:
@@ -246,6 +247,8 @@ def run_ours(args):
     ctx.check(lib.lamb_probe_fp64_tflops(local, 5, ctypes.byref(peak)))
     fp64_peak = peak.value
     da, db = ctx.upload(a), ctx.upload(b)
+    if not args.no_positions:
+        da.set_positions(g.sector_positions(), g.box)
     dc = ctx.create_like(da)
     ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local))
     for _ in range(args.warmup):
@@ -284,6 +287,7 @@ def run_ours(args):
     # e2e through the C ABI with page-locked host buffers
     pa, pb = pin_matrix(a), pin_matrix(b)
     c_out = dc.download(pinned=True)
+    pos = g.sector_positions()
     h2d = matrix_bytes(pa) + matrix_bytes(pb)
     d2h = matrix_bytes(c_out)
     barrier()
@@ -292,6 +296,8 @@ def run_ours(args):
         torch.cuda.synchronize()
         t = time.perf_counter()
         xa, xb = ctx.upload(pa), ctx.upload(pb)
+        if not args.no_positions:
+            xa.set_positions(pos, g.box)
         xc = ctx.create_like(xa)
         st_e = ctx.multiply(xa, xb, xc, wl.eps)
         c_out = xc.download(out=c_out)
@@ -316,7 +322,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water boxes)",
             "config": {"workload": wl.name, "n_mol": wl.n_mol, "n_atoms": g.n_atoms, "box": wl.box,
-                       "cutoff": wl.cutoff, "eps": wl.eps, "path": "plain FP64 (DMMA)",
+                       "cutoff": wl.cutoff, "eps": wl.eps, "path": "plain FP64 (DMMA)", "row_order": "pattern (Cuthill-McKee)" if args.no_positions else "Morton (atom coordinates)",
                        "l2": "inputs 2x1.9 GB exceed L2; no flush", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "tensor", "kernel": "k_numeric_fp64", "achieved": achieved_tf,
                          "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak,

@@ -165,6 +165,16 @@ LAMB_API int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* ctx, const lamb_c_sector* 
  * lamb_matrix_copy + clearing gives the reference's C argument). */
 LAMB_API int32_t lamb_gpu_matrix_create_like(lamb_gpu_ctx* ctx, lamb_gpu_matrix like, lamb_gpu_matrix* handle);
 LAMB_API int32_t lamb_gpu_matrix_destroy(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle);
+/* Optional locality hint: coordinates of the row atoms in sector order
+ * (xyz[3*n_rows], subset 1's atoms in local order first) and the orthorhombic
+ * cell lengths (box[3]).  LAMB's distributions carry these coordinates
+ * (lamb_set coordinates, real_4, src/lamb_set_partition_methods.F90:69-144);
+ * the multiply uses them only to order its work along a Morton curve so that
+ * concurrently processed C rows share B rows in L2.  Without the hint a
+ * Cuthill-McKee order of the block pattern is used.  Results do not depend
+ * on the order. */
+LAMB_API int32_t lamb_gpu_matrix_set_positions(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, const float* xyz,
+                                               int32_t n_rows, const float* box);
 /* Number of sectors, then per-sector sizes (sizes[n_sectors]). */
 LAMB_API int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, int32_t* n_sectors);
 LAMB_API int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_sizes* sizes,

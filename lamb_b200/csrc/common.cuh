@@ -42,10 +42,12 @@ struct DevMatrix {
   double* data = nullptr;      // [data_len]
   double* norms = nullptr;     // [nnz] Frobenius norms, valid when norms_valid
   bool norms_valid = false;
-  // For uploaded matrices: source sector and block id of every global block
-  // (used to express stacks in the caller's numbering).
-  int32_t* src_sec = nullptr;  // [nnz]
-  int64_t* src_blk = nullptr;  // [nnz]
+  // Locality: optional row-atom coordinates (sector order) and the processing
+  // order of rows derived from them (Morton) or from the pattern (Cuthill-McKee).
+  std::vector<float> h_pos;    // 3*n_rows, empty when not given
+  float box[3] = {0, 0, 0};
+  std::vector<int32_t> h_order;  // row processing order, empty until computed
+  int32_t* order = nullptr;      // device copy of h_order
 };
 
 struct Ctx {
@@ -99,6 +101,11 @@ DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h);
 void free_matrix_buffers(Ctx* ctx, DevMatrix* m);
 int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h);
 int32_t ensure_norms(Ctx* ctx, DevMatrix* m);
+// Row processing order of m (computed once, cached): Morton order of the row
+// coordinates when given, else Cuthill-McKee order of m's block pattern.
+int32_t ensure_row_order(Ctx* ctx, DevMatrix* m);
+// Copies the row locality data (coordinates and order) of src to dst.
+int32_t inherit_row_locality(Ctx* ctx, DevMatrix* dst, const DevMatrix* src);
 // Copies the subset structure (not the blocks) of rows of `r` and columns of `c`.
 void copy_structure(DevMatrix* dst, const DevMatrix* r_src, bool rows_from_rows, const DevMatrix* c_src,
                     bool cols_from_cols);

@@ -32,8 +32,8 @@ void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
   dfree(ctx, m->off);
   dfree(ctx, m->data);
   dfree(ctx, m->norms);
-  dfree(ctx, m->src_sec);
-  dfree(ctx, m->src_blk);
+  dfree(ctx, m->order);
+  m->h_order.clear();
   m->norms_valid = false;
 }
 
@@ -250,6 +250,106 @@ int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of) {
   return LAMB_GPU_OK;
 }
 
+// ---- row processing order ------------------------------------------------------------
+// Morton (Z-order) key of a point in the periodic cell, 10 bits per axis.
+static uint32_t morton3(float x, float y, float z, const float* box) {
+  auto q = [](float v, float L) {
+    float f = v / L;
+    f -= floorf(f);
+    int c = (int)(f * 1024.0f);
+    return (uint32_t)(c < 0 ? 0 : (c > 1023 ? 1023 : c));
+  };
+  auto spread = [](uint32_t v) {
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+  };
+  return spread(q(x, box[0])) | (spread(q(y, box[1])) << 1) | (spread(q(z, box[2])) << 2);
+}
+
+// Cuthill-McKee: BFS from a pseudo-peripheral row, neighbours by increasing
+// degree.  Uses the block pattern as a graph (columns index the same atoms as
+// rows when the matrix is square in atoms).
+static void cuthill_mckee(int n, const std::vector<int64_t>& rp, const std::vector<int32_t>& cl,
+                          std::vector<int32_t>& order) {
+  order.clear();
+  order.reserve(n);
+  std::vector<int32_t> deg(n), level(n, -1);
+  for (int i = 0; i < n; ++i) deg[i] = (int32_t)(rp[i + 1] - rp[i]);
+  auto bfs_last = [&](int s) {
+    std::vector<int32_t> q{s};
+    std::fill(level.begin(), level.end(), -1);
+    level[s] = 0;
+    for (size_t h = 0; h < q.size(); ++h)
+      for (int64_t b = rp[q[h]]; b < rp[q[h] + 1]; ++b) {
+        int j = cl[b];
+        if (j < n && level[j] < 0) { level[j] = level[q[h]] + 1; q.push_back(j); }
+      }
+    return q.back();
+  };
+  std::vector<char> seen(n, 0);
+  std::vector<int32_t> nb;
+  for (int start = 0; start < n; ++start) {
+    if (seen[start]) continue;
+    int s = bfs_last(bfs_last(start));
+    if (seen[s]) s = start;
+    size_t h = order.size();
+    order.push_back(s);
+    seen[s] = 1;
+    for (; h < order.size(); ++h) {
+      nb.clear();
+      for (int64_t b = rp[order[h]]; b < rp[order[h] + 1]; ++b) {
+        int j = cl[b];
+        if (j < n && !seen[j]) { seen[j] = 1; nb.push_back(j); }
+      }
+      std::sort(nb.begin(), nb.end(), [&](int x, int y) { return deg[x] < deg[y] || (deg[x] == deg[y] && x < y); });
+      order.insert(order.end(), nb.begin(), nb.end());
+    }
+  }
+}
+
+int32_t ensure_row_order(Ctx* ctx, DevMatrix* m) {
+  if (!m->h_order.empty() || m->n_rows == 0) {
+    if (m->n_rows && !m->order) {
+      LAMB_TRY(dalloc(ctx, &m->order, m->n_rows));
+      LAMB_CUDA(ctx, cudaMemcpyAsync(m->order, m->h_order.data(), sizeof(int32_t) * m->n_rows,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return LAMB_GPU_OK;
+  }
+  const int n = m->n_rows;
+  std::vector<int32_t> ord(n);
+  if ((int64_t)m->h_pos.size() == 3ll * n) {
+    std::vector<std::pair<uint32_t, int32_t>> key(n);
+    for (int i = 0; i < n; ++i) key[i] = {morton3(m->h_pos[3 * i], m->h_pos[3 * i + 1], m->h_pos[3 * i + 2], m->box), i};
+    std::sort(key.begin(), key.end());
+    for (int i = 0; i < n; ++i) ord[i] = key[i].second;
+  } else if (m->n_cols == m->n_rows && m->nnz > 0) {
+    std::vector<int64_t> rp(n + 1);
+    std::vector<int32_t> cl(m->nnz);
+    LAMB_CUDA(ctx, cudaMemcpyAsync(rp.data(), m->row_p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(cl.data(), m->col, sizeof(int32_t) * m->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cuthill_mckee(n, rp, cl, ord);
+  } else {
+    for (int i = 0; i < n; ++i) ord[i] = i;
+  }
+  m->h_order.swap(ord);
+  dfree(ctx, m->order);
+  return ensure_row_order(ctx, m);
+}
+
+int32_t inherit_row_locality(Ctx* ctx, DevMatrix* dst, const DevMatrix* src) {
+  if (dst->n_rows != src->n_rows) return LAMB_GPU_OK;
+  dst->h_pos = src->h_pos;
+  memcpy(dst->box, src->box, sizeof(dst->box));
+  dst->h_order = src->h_order;
+  dfree(ctx, dst->order);
+  return LAMB_GPU_OK;
+}
+
 // ---- sector structure validation ------------------------------------------------
 static int32_t check_sector(Ctx* ctx, const lamb_c_sector& s, int idx) {
   auto bad = [&](const std::string& w) {
@@ -423,8 +523,7 @@ int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_
   m->data_len = dpos;
   m->nnz = nnz;
   std::vector<int64_t> h_row_p(m->n_rows + 1, 0), h_off(nnz);
-  std::vector<int32_t> h_col(nnz), h_src(nnz);
-  std::vector<int64_t> h_srcb(nnz);
+  std::vector<int32_t> h_col(nnz);
   int64_t p = 0;
   for (int a = 0; a < R; ++a)
     for (int l = 0; l < m->rsub_cnt[a]; ++l) {
@@ -436,8 +535,6 @@ int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_
           h_col[p] = m->csub_base[n] + s.col_i[b] - 1;
           const int64_t sz = s.extents[2 * b + 1] - s.extents[2 * b] + 1;
           h_off[p] = m->sec_base[(size_t)a * S + n] + (sz > 0 ? s.extents[2 * b] - 1 : 0);
-          h_src[p] = i;
-          h_srcb[p] = b;
           ++p;
         }
       }
@@ -447,15 +544,11 @@ int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_
   LAMB_TRY(dalloc(ctx, &m->row_p, m->n_rows + 1));
   LAMB_TRY(dalloc(ctx, &m->col, std::max<int64_t>(nnz, 1)));
   LAMB_TRY(dalloc(ctx, &m->off, std::max<int64_t>(nnz, 1)));
-  LAMB_TRY(dalloc(ctx, &m->src_sec, std::max<int64_t>(nnz, 1)));
-  LAMB_TRY(dalloc(ctx, &m->src_blk, std::max<int64_t>(nnz, 1)));
   LAMB_TRY(dalloc(ctx, &m->data, std::max<int64_t>(m->data_len, 1)));
   LAMB_CUDA(ctx, cudaMemcpyAsync(m->row_p, h_row_p.data(), sizeof(int64_t) * (m->n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
   if (nnz) {
     LAMB_CUDA(ctx, cudaMemcpyAsync(m->col, h_col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(m->off, h_off.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(m->src_sec, h_src.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(m->src_blk, h_srcb.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
   }
   for (size_t k = 0; k < sid.size(); ++k)
     if (sid[k] >= 0 && sec[sid[k]].data_len > 0)
@@ -491,6 +584,23 @@ int32_t lamb_gpu_matrix_destroy(lamb_gpu_ctx* c, lamb_gpu_matrix h) {
   cudaSetDevice(ctx->device);
   free_matrix_buffers(ctx, it->second.get());
   ctx->mats.erase(it);
+  return LAMB_GPU_OK;
+}
+
+int32_t lamb_gpu_matrix_set_positions(lamb_gpu_ctx* c, lamb_gpu_matrix h, const float* xyz, int32_t n_rows,
+                                      const float* box) {
+  auto* ctx = reinterpret_cast<Ctx*>(c);
+  if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  DevMatrix* m = get_matrix(ctx, h);
+  if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "set_positions: invalid handle");
+  if (!xyz || !box || n_rows != m->n_rows)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "set_positions: need 3*n_rows coordinates and box[3]");
+  for (int d = 0; d < 3; ++d)
+    if (!(box[d] > 0)) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "set_positions: box must be positive");
+  m->h_pos.assign(xyz, xyz + 3 * (size_t)n_rows);
+  memcpy(m->box, box, sizeof(m->box));
+  m->h_order.clear();
+  dfree(ctx, m->order);
   return LAMB_GPU_OK;
 }
 

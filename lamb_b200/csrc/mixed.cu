@@ -3,8 +3,8 @@
 
 namespace lamb {
 
-int32_t numeric_mixed(Ctx* ctx, DevMatrix*, DevMatrix*, DevMatrix*, const Symbolic&, const int64_t*, double*,
-                      int* slices_used) {
+int32_t numeric_mixed(Ctx* ctx, DevMatrix*, DevMatrix*, DevMatrix*, const Symbolic&, const Work*, const int32_t*,
+                      double*, int* slices_used) {
   *slices_used = 0;
   return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "mixed precision not built yet");
 }

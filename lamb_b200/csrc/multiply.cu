@@ -19,7 +19,8 @@ namespace lamb {
 
 void free_symbolic(Ctx* ctx, Symbolic& s) {
   dfree(ctx, s.stack_p);
-  dfree(ctx, s.stack);
+  dfree(ctx, s.ent);
+  dfree(ctx, s.ids);
   dfree(ctx, s.c_row);
 }
 
@@ -118,12 +119,14 @@ __device__ __forceinline__ int bm_rank(const uint32_t* bm, const int* wpre, int 
   return wpre[j >> 5] + __popc(bm[j >> 5] & ((1u << (j & 31)) - 1u));
 }
 
+template <bool IDS>
 __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
     const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
     const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, const int64_t* __restrict__ c_row_p,
     const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col, int64_t* __restrict__ stack_p,
-    int2* __restrict__ stack) {
+    const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off, Ent* __restrict__ ent,
+    int2* __restrict__ ids) {
   extern __shared__ uint32_t sm[];
   uint32_t* bm = sm;
   int* wpre = (int*)(sm + n_words);
@@ -176,28 +179,36 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     for (int64_t ab = a0; ab < a1; ++ab) {
       const int k = a_col[ab];
       const double na = a_nrm[ab];
+      const long long ak = IDS ? 0 : a_offk[ab];
       for (int64_t bb = b_row_p[k] + tid; bb < b_row_p[k + 1]; bb += kSymThreads)
         if (keep_pair(na, b_nrm[bb], eps, filt)) {
           const int p = bm_rank(bm, wpre, b_col[bb]);
           const int slot = cur[p];
           cur[p] = slot + 1;
-          stack[sb + slot] = make_int2((int)ab, (int)bb);
+          if (IDS)
+            ids[sb + slot] = make_int2((int)ab, (int)bb);
+          else
+            ent[sb + slot] = Ent{ak, (long long)b_off[bb]};
         }
       __syncthreads();
     }
   }
 }
 
-int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, Symbolic* out) {
-  *out = Symbolic{};
+int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, bool want_ids,
+                       const int64_t* a_offk, Symbolic* out) {
+  out->c_nnz = out->n_ent = out->n_pairs = 0;
+  out->flops = 0;
   LAMB_TRY(check_compatible(ctx, A, B));
   LAMB_TRY(ensure_norms(ctx, A));
   LAMB_TRY(ensure_norms(ctx, B));
   if (A->nnz >= (1ll << 31) || B->nnz >= (1ll << 31))
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "more than 2^31 blocks in an operand");
+  if (!want_ids && !a_offk) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "symbolic: no A meta");
   // C takes A's row subsets and B's column subsets.
   free_matrix_buffers(ctx, C);
   copy_structure(C, A, true, B, true);
+  LAMB_TRY(inherit_row_locality(ctx, C, A));
   LAMB_TRY(upload_block_sizes(ctx, C));
   const int32_t n_rows = C->n_rows;
   const int32_t n_words = (C->n_cols + 31) / 32;
@@ -221,27 +232,29 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
         n_words, c_cnt, s_cnt, p_cnt, rfl);
     LAMB_LAUNCHED(ctx);
   }
-  std::vector<int64_t> h_c(n_rows), h_s(n_rows), h_p(n_rows);
+  std::vector<int64_t> h_s(n_rows), h_p(n_rows);
   std::vector<double> h_f(n_rows);
+  out->h_row_len.assign(n_rows, 0);
   if (n_rows) {
-    LAMB_CUDA(ctx, cudaMemcpyAsync(h_c.data(), c_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(out->h_row_len.data(), c_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_s.data(), s_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_p.data(), p_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_f.data(), rfl, sizeof(double) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   std::vector<int64_t> h_crp(n_rows + 1, 0), h_srb(n_rows + 1, 0);
-  int64_t max_c = 0;
+  int64_t max_c = 0, max_s = 0;
   for (int r = 0; r < n_rows; ++r) {
-    h_crp[r + 1] = h_crp[r] + h_c[r];
+    h_crp[r + 1] = h_crp[r] + out->h_row_len[r];
     h_srb[r + 1] = h_srb[r] + h_s[r];
     out->n_pairs += h_p[r];
     out->flops += h_f[r];
-    max_c = std::max(max_c, h_c[r]);
+    max_c = std::max(max_c, out->h_row_len[r]);
+    max_s = std::max(max_s, h_s[r]);
   }
   out->c_nnz = h_crp[n_rows];
   out->n_ent = h_srb[n_rows];
-  if (out->n_ent >= (1ll << 40))
+  if (out->n_ent >= (1ll << 40) || max_s >= (1ll << 24))
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "stack too large");
   C->nnz = out->c_nnz;
   int64_t* s_row_base = nullptr;
@@ -250,215 +263,89 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_CUDA(ctx, cudaMemcpyAsync(s_row_base, h_srb.data(), sizeof(int64_t) * (n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
   LAMB_TRY(dalloc(ctx, &C->col, std::max<int64_t>(C->nnz, 1)));
   LAMB_TRY(dalloc(ctx, &out->stack_p, C->nnz + 1));
-  LAMB_TRY(dalloc(ctx, &out->stack, std::max<int64_t>(out->n_ent, 1)));
+  if (want_ids)
+    LAMB_TRY(dalloc(ctx, &out->ids, std::max<int64_t>(out->n_ent, 1)));
+  else
+    LAMB_TRY(dalloc(ctx, &out->ent, std::max<int64_t>(out->n_ent, 1)));
   LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
   const size_t smem_fill = sizeof(uint32_t) * (size_t)std::max(n_words, 1) * 2 + sizeof(int) * (size_t)(max_c + 1);
   if (smem_fill > 220 * 1024)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
   if (n_rows > 0 && C->nnz > 0) {
+    auto kern = want_ids ? k_sym_fill<true> : k_sym_fill<false>;
     if (smem_fill > 48 * 1024)
-      LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
-    k_sym_fill<<<grid, kSymThreads, smem_fill, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col,
-                                                               B->norms, eps, fl, n_words, C->row_p, s_row_base,
-                                                               C->col, out->stack_p, out->stack);
+      LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
+    kern<<<grid, kSymThreads, smem_fill, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms,
+                                                        eps, fl, n_words, C->row_p, s_row_base, C->col, out->stack_p,
+                                                        a_offk, B->off, out->ent, out->ids);
     LAMB_LAUNCHED(ctx);
   }
   LAMB_TRY(dalloc(ctx, &out->c_row, std::max<int64_t>(C->nnz, 1)));
   LAMB_TRY(layout_sector_major(ctx, C, out->c_row));
+  if (C->data_len >= kMask40) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C data too large");
   LAMB_TRY(dalloc(ctx, &C->data, std::max<int64_t>(C->data_len, 1)));
   dfree(ctx, c_cnt); dfree(ctx, s_cnt); dfree(ctx, p_cnt); dfree(ctx, rfl); dfree(ctx, s_row_base);
   return LAMB_GPU_OK;
 }
 
-// ---- A meta: data offset and k block size in one word -----------------------------
-__global__ void k_pack_a_meta(int64_t nnz, const int32_t* __restrict__ col, const int64_t* __restrict__ off,
-                              const int8_t* __restrict__ col_bs, int64_t* __restrict__ out) {
-  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nnz; b += (int64_t)gridDim.x * blockDim.x)
-    out[b] = off[b] | ((int64_t)col_bs[col[b]] << 56);
+// ---- operand meta: data offset and inner block size in one word ------------------------
+__global__ void k_pack_offk(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                            const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                            const int8_t* __restrict__ col_bs, int k_is_col, int64_t* __restrict__ out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b)
+      out[b] = off[b] | ((int64_t)(k_is_col ? col_bs[col[b]] : row_bs[r]) << 56);
 }
 
-int32_t pack_a_meta(Ctx* ctx, const DevMatrix* A, int64_t** a_offk) {
-  LAMB_TRY(dalloc(ctx, a_offk, std::max<int64_t>(A->nnz, 1)));
-  if (A->data_len > kOffMask) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "A data too large");
-  if (A->nnz) {
-    k_pack_a_meta<<<grid_for(A->nnz), kThreads, 0, ctx->stream>>>(A->nnz, A->col, A->off, A->col_bs, *a_offk);
+int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk) {
+  LAMB_TRY(dalloc(ctx, offk, std::max<int64_t>(m->nnz, 1)));
+  if (m->data_len > kOffMask) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "operand data too large");
+  if (m->nnz) {
+    k_pack_offk<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->off, m->row_bs,
+                                                                     m->col_bs, k_is_col ? 1 : 0, *offk);
     LAMB_LAUNCHED(ctx);
   }
   return LAMB_GPU_OK;
 }
 
-// ---- FP64 numeric phase ---------------------------------------------------------------
-// One warp owns one C block (segment ownership: no atomics).  The block's
-// stack is consumed as one concatenated K dimension: sum_e A_ik(e) . B_k(e)j
-// = [A_ik1 | A_ik2 | ...] . [B_k1j; B_k2j; ...], padded to a multiple of 4
-// once per 32 entries instead of once per entry.  Products run on the FP64
-// tensor pipe with mma.m8n8k4 (DMMA): MF x NF fragments of 8x8 cover the
-// b_i x b_j block.  Fragment layouts (PTX ISA, mma.m8n8k4 .f64):
-//   A (8x4, row): lane holds A[lane/4][lane%4]
-//   B (4x8, col): lane holds B[lane%4][lane/4]
-//   C (8x8):      lane holds C[lane/4][2*(lane%4) + {0,1}]
-constexpr int kNumWarps = 8;
-
-struct WarpMeta {
-  long long ao[32];
-  long long bo[32];
-  int pre[33];
-};
-
-__device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
-}
-
-template <int MF, int NF>
-__device__ __forceinline__ void cblock_fp64(const double* __restrict__ Ad, const double* __restrict__ Bd,
-                                            double* __restrict__ Cd, int bi, int bj, int64_t c_off, int64_t s0,
-                                            int64_t s1, const int2* __restrict__ stk,
-                                            const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off,
-                                            WarpMeta& wm, double* __restrict__ c_nrm, int64_t c) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  double acc[MF][NF][2];
-#pragma unroll
-  for (int i = 0; i < MF; ++i)
-#pragma unroll
-    for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  for (int64_t base = s0; base < s1; base += 32) {
-    const int n = (int)min((int64_t)32, s1 - base);
-    int bk = 0;
-    long long ao = 0, bo = 0;
-    if (lane < n) {
-      const int2 e = stk[base + lane];
-      const long long ak = a_offk[e.x];
-      ao = ak & kOffMask;
-      bk = (int)(ak >> 56);
-      bo = b_off[e.y];
-    }
-    const int incl = warp_incl_scan(bk, lane);
-    wm.ao[lane] = ao;
-    wm.bo[lane] = bo;
-    wm.pre[lane] = incl - bk;
-    if (lane == 31) wm.pre[32] = incl;
-    __syncwarp();
-    const int K = wm.pre[32];
-    int e = 0;
-    for (int kw = 0; kw < K; kw += 4) {
-      const int colk = kw + t;
-      while (e < n - 1 && colk >= wm.pre[e + 1]) ++e;
-      const bool valid = colk < K;
-      const int kc = colk - wm.pre[e];
-      const int bke = wm.pre[e + 1] - wm.pre[e];
-      const double* pa = Ad + wm.ao[e] + (int64_t)kc * bi;
-      const double* pb = Bd + wm.bo[e] + kc;
-      double av[MF], bv[NF];
-#pragma unroll
-      for (int i = 0; i < MF; ++i) {
-        const int r = i * 8 + g;
-        av[i] = (valid && r < bi) ? __ldg(pa + r) : 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < NF; ++j) {
-        const int cc = j * 8 + g;
-        bv[j] = (valid && cc < bj) ? __ldg(pb + (int64_t)cc * bke) : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < MF; ++i)
-#pragma unroll
-        for (int j = 0; j < NF; ++j) dmma884(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
-    }
-    __syncwarp();
-  }
-  double sq = 0.0;
-#pragma unroll
-  for (int i = 0; i < MF; ++i)
-#pragma unroll
-    for (int j = 0; j < NF; ++j)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = i * 8 + g, cc = j * 8 + 2 * t + h;
-        if (r < bi && cc < bj) {
-          const double v = acc[i][j][h];
-          Cd[c_off + (int64_t)cc * bi + r] = v;
-          sq = __fma_rn(v, v, sq);
-        }
-      }
-  sq = warp_sum(sq);
-  if (lane == 0 && c_nrm) c_nrm[c] = __dsqrt_rn(sq);
-}
-
-// Generic path for blocks wider than 24 rows or columns: plain FP64 FMAs,
-// one C element per lane and step.
-__device__ void cblock_fp64_generic(const double* __restrict__ Ad, const double* __restrict__ Bd,
-                                    double* __restrict__ Cd, int bi, int bj, int64_t c_off, int64_t s0, int64_t s1,
-                                    const int2* __restrict__ stk, const int64_t* __restrict__ a_offk,
-                                    const int64_t* __restrict__ b_off, double* __restrict__ c_nrm, int64_t c) {
-  const int lane = threadIdx.x & 31;
-  double sq = 0.0;
-  for (int el = lane; el < bi * bj; el += 32) {
-    const int r = el % bi, cc = el / bi;
-    double acc = 0.0;
-    for (int64_t s = s0; s < s1; ++s) {
-      const int2 e = stk[s];
-      const long long ak = a_offk[e.x];
-      const int bk = (int)(ak >> 56);
-      const double* pa = Ad + (ak & kOffMask);
-      const double* pb = Bd + b_off[e.y];
-      for (int kk = 0; kk < bk; ++kk) acc = __fma_rn(pa[(int64_t)kk * bi + r], pb[(int64_t)cc * bk + kk], acc);
-    }
-    Cd[c_off + (int64_t)cc * bi + r] = acc;
-    sq = __fma_rn(acc, acc, sq);
-  }
-  sq = warp_sum(sq);
-  if (lane == 0 && c_nrm) c_nrm[c] = __dsqrt_rn(sq);
-}
-
-__global__ void __launch_bounds__(kNumWarps * 32) k_numeric_fp64(
-    int64_t c_nnz, const int32_t* __restrict__ c_row, const int32_t* __restrict__ c_col,
-    const int64_t* __restrict__ c_off, const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs,
-    const int64_t* __restrict__ stack_p, const int2* __restrict__ stk, const int64_t* __restrict__ a_offk,
-    const int64_t* __restrict__ b_off, const double* __restrict__ Ad, const double* __restrict__ Bd,
-    double* __restrict__ Cd, double* __restrict__ c_nrm) {
-  __shared__ WarpMeta wms[kNumWarps];
-  const int w = threadIdx.x >> 5;
-  WarpMeta& wm = wms[w];
-  const int64_t nwarps = (int64_t)gridDim.x * kNumWarps;
-  for (int64_t c = (int64_t)blockIdx.x * kNumWarps + w; c < c_nnz; c += nwarps) {
-    const int bi = row_bs[c_row[c]], bj = col_bs[c_col[c]];
-    const int64_t co = c_off[c], s0 = stack_p[c], s1 = stack_p[c + 1];
-    const int mf = (bi + 7) >> 3, nf = (bj + 7) >> 3;
-    switch (mf * 4 + nf) {
-      case 0 * 4 + 0: case 0 * 4 + 1: case 0 * 4 + 2: case 0 * 4 + 3: case 1 * 4 + 0: case 2 * 4 + 0:
-      case 3 * 4 + 0:  // a zero-size block: no data, norm 0
-        if ((threadIdx.x & 31) == 0 && c_nrm) c_nrm[c] = 0.0;
-        break;
-      case 1 * 4 + 1: cblock_fp64<1, 1>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 1 * 4 + 2: cblock_fp64<1, 2>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 1 * 4 + 3: cblock_fp64<1, 3>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 2 * 4 + 1: cblock_fp64<2, 1>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 2 * 4 + 2: cblock_fp64<2, 2>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 2 * 4 + 3: cblock_fp64<2, 3>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 3 * 4 + 1: cblock_fp64<3, 1>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 3 * 4 + 2: cblock_fp64<3, 2>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      case 3 * 4 + 3: cblock_fp64<3, 3>(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, wm, c_nrm, c); break;
-      default: cblock_fp64_generic(Ad, Bd, Cd, bi, bj, co, s0, s1, stk, a_offk, b_off, c_nrm, c); break;
+// ---- work list in the row processing order --------------------------------------------
+__global__ void k_build_work(int32_t n_rows, const int32_t* __restrict__ order, const int64_t* __restrict__ cum,
+                             const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                             const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                             const int8_t* __restrict__ col_bs, const int64_t* __restrict__ stack_p,
+                             Work* __restrict__ work, int32_t* __restrict__ work_c) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n_rows; w += (int64_t)gridDim.x * blockDim.x) {
+    const int r = order[w];
+    const long long bi = row_bs[r];
+    int64_t v = cum[w];
+    for (int64_t c = row_p[r]; c < row_p[r + 1]; ++c, ++v) {
+      const long long bj = col_bs[col[c]];
+      const long long n = stack_p[c + 1] - stack_p[c];
+      work[v] = Work{(long long)off[c] | (bi << 40) | (bj << 48), (long long)stack_p[c] | (n << 40)};
+      work_c[v] = (int32_t)c;
     }
   }
 }
 
-int32_t numeric_fp64(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, DevMatrix* C, const Symbolic& sym,
-                     const int64_t* a_offk, double* c_nrm) {
-  if (sym.c_nnz == 0) return LAMB_GPU_OK;
-  int dev_sms = 148;
-  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  int per_sm = 0;
-  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_numeric_fp64, kNumWarps * 32, 0));
-  const int64_t need = (sym.c_nnz + kNumWarps - 1) / kNumWarps;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)dev_sms * std::max(per_sm, 1)));
-  k_numeric_fp64<<<grid, kNumWarps * 32, 0, ctx->stream>>>(sym.c_nnz, sym.c_row, C->col, C->off, C->row_bs,
-                                                            C->col_bs, sym.stack_p, sym.stack, a_offk, B->off,
-                                                            A->data, B->data, C->data, c_nrm);
+int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
+                   int32_t** work_c) {
+  const int n = C->n_rows;
+  LAMB_TRY(dalloc(ctx, work, std::max<int64_t>(sym.c_nnz, 1)));
+  LAMB_TRY(dalloc(ctx, work_c, std::max<int64_t>(sym.c_nnz, 1)));
+  if (sym.c_nnz == 0 || n == 0) return LAMB_GPU_OK;
+  if ((int)order_src->h_order.size() != n || !order_src->order)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "work list: row order missing");
+  std::vector<int64_t> cum(n + 1, 0);
+  for (int w = 0; w < n; ++w) cum[w + 1] = cum[w] + sym.h_row_len[order_src->h_order[w]];
+  int64_t* d_cum = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_cum, n + 1));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cum, cum.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, ctx->stream));
+  k_build_work<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, d_cum, C->row_p, C->col, C->off,
+                                                            C->row_bs, C->col_bs, sym.stack_p, *work, *work_c);
   LAMB_LAUNCHED(ctx);
+  // cum must outlive the launch: stream-ordered free.
+  dfree(ctx, d_cum);
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return LAMB_GPU_OK;
 }
 
@@ -551,27 +438,34 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   const int64_t launches0 = ctx->launches;
   if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
   Symbolic sym;
-  int32_t rc = symbolic_phase(ctx, A, B, C, eps, filt_p, &sym);
-  if (rc != LAMB_GPU_OK) { free_symbolic(ctx, sym); return rc; }
-  if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
   int64_t* a_offk = nullptr;
   double* c_nrm = nullptr;
-  rc = pack_a_meta(ctx, A, &a_offk);
-  if (rc == LAMB_GPU_OK) rc = dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1));
-  if (rc == LAMB_GPU_OK && timed) rc = cudaEventRecord(ctx->ev[2], ctx->stream) == cudaSuccess ? 0 : rc;
+  Work* work = nullptr;
+  int32_t* work_c = nullptr;
   int slices = 0;
-  if (rc == LAMB_GPU_OK) {
-    if (flags & LAMB_GPU_MIXED)
-      rc = numeric_mixed(ctx, A, B, C, sym, a_offk, c_nrm, &slices);
-    else
-      rc = numeric_fp64(ctx, A, B, C, sym, a_offk, c_nrm);
-  }
-  if (rc == LAMB_GPU_OK && timed) rc = cudaEventRecord(ctx->ev[3], ctx->stream) == cudaSuccess ? 0 : rc;
   int64_t dropped = 0;
-  if (rc == LAMB_GPU_OK && filt_r) rc = result_filter(ctx, C, c_nrm, eps, &dropped);
-  if (rc == LAMB_GPU_OK && timed) rc = cudaEventRecord(ctx->ev[4], ctx->stream) == cudaSuccess ? 0 : rc;
+  auto body = [&]() -> int32_t {
+    LAMB_TRY(check_compatible(ctx, A, B));
+    LAMB_TRY(ensure_row_order(ctx, A));
+    LAMB_TRY(pack_offk(ctx, A, true, &a_offk));
+    LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
+    LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c));
+    LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
+    if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    if (flags & LAMB_GPU_MIXED)
+      LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, &slices));
+    else
+      LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false));
+    if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps, &dropped));
+    if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    return LAMB_GPU_OK;
+  };
+  int32_t rc = body();
   dfree(ctx, a_offk);
   dfree(ctx, c_nrm);
+  dfree(ctx, work);
+  dfree(ctx, work_c);
   free_symbolic(ctx, sym);
   if (rc != LAMB_GPU_OK) return rc;
   C->norms_valid = false;
@@ -583,14 +477,14 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   st.mixed_slices = slices;
   st.kernel_launches = (int32_t)(ctx->launches - launches0);
   if (timed) {
-    LAMB_CUDA(ctx, cudaEventSynchronize(ctx->ev[4]));
-    float t01 = 0, t23 = 0, t04 = 0;
+    LAMB_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    float t01 = 0, t12 = 0, t03 = 0;
     cudaEventElapsedTime(&t01, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&t23, ctx->ev[2], ctx->ev[3]);
-    cudaEventElapsedTime(&t04, ctx->ev[0], ctx->ev[4]);
+    cudaEventElapsedTime(&t12, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&t03, ctx->ev[0], ctx->ev[3]);
     st.ms_symbolic = t01;
-    st.ms_numeric = t23;
-    st.ms_total = t04;
+    st.ms_numeric = t12;
+    st.ms_total = t03;
   }
   ctx->last_stats = st;
   if (stats) *stats = st;
@@ -636,7 +530,7 @@ static int32_t stacks_export(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C,
   LAMB_TRY(d2h_csr(C, crp, ccl));
   LAMB_CUDA(ctx, cudaMemcpyAsync(sp.data(), sym.stack_p, sizeof(int64_t) * (sym.c_nnz + 1), cudaMemcpyDeviceToHost, ctx->stream));
   if (sym.n_ent)
-    LAMB_CUDA(ctx, cudaMemcpyAsync(st.data(), sym.stack, sizeof(int2) * sym.n_ent, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(st.data(), sym.ids, sizeof(int2) * sym.n_ent, cudaMemcpyDeviceToHost, ctx->stream));
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (!entries) { *n_entries = sym.n_ent; return LAMB_GPU_OK; }
   if (*n_entries < sym.n_ent) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "stacks: capacity too small");
@@ -706,7 +600,7 @@ int32_t lamb_gpu_multiply_stacks(lamb_gpu_ctx* c, lamb_gpu_matrix a, lamb_gpu_ma
   cudaSetDevice(ctx->device);
   const bool filt_p = eps > 0 && !(flags & LAMB_GPU_NO_PRODUCT_FILTER);
   Symbolic sym;
-  int32_t rc = symbolic_phase(ctx, A, B, C, eps, filt_p, &sym);
+  int32_t rc = symbolic_phase(ctx, A, B, C, eps, filt_p, true, nullptr, &sym);
   if (rc == LAMB_GPU_OK) rc = stacks_export(ctx, A, B, C, sym, entries, n_entries);
   free_symbolic(ctx, sym);
   return rc;

@@ -4,37 +4,63 @@
 
 namespace lamb {
 
-// Output of the symbolic phase.  The stack of C block c is
-// stack[stack_p[c] .. stack_p[c+1]), pairs (A block id, B block id) of the
-// global CSRs, ordered by k ascending in sector order, i.e. by (k subset,
-// local k) -- the canonical order of the build's stacks.
+constexpr int64_t kOffMask = (1ll << 56) - 1;
+constexpr int64_t kMask40 = (1ll << 40) - 1;
+
+// One resolved stack entry: the two operand blocks of a block product.
+//   a = data offset of operand 1 | (inner block size << 56)
+//   b = data offset of operand 2
+struct Ent {
+  long long a;
+  long long b;
+};
+
+// One unit of numeric work (a C block), in the processing order:
+//   lo = C data offset (40 bits) | rows << 40 | cols << 48
+//   hi = first stack entry (40 bits) | entry count << 40
+struct Work {
+  long long lo;
+  long long hi;
+};
+
+// Output of the symbolic phase.  The stack of C block c is the entry range
+// [stack_p[c], stack_p[c+1]), ordered by k ascending in sector order, i.e. by
+// (k subset, local k): the canonical order of the build's stacks.  Entries are
+// stored resolved (`ent`, for the numeric kernels) or as block-id pairs
+// (`ids`, (A block, B block) of the global CSRs, for exporting stacks).
 struct Symbolic {
   int64_t c_nnz = 0;
   int64_t n_ent = 0;
   int64_t n_pairs = 0;  // products before the product filter
   double flops = 0;     // sum of 2*b_i*b_k*b_j over the stack
   int64_t* stack_p = nullptr;  // [c_nnz+1]
-  int2* stack = nullptr;       // [n_ent]
+  Ent* ent = nullptr;          // [n_ent] when resolved
+  int2* ids = nullptr;         // [n_ent] when ids were requested
   int32_t* c_row = nullptr;    // [c_nnz] row of every C block
-  int32_t max_stack = 0;       // longest stack of one C block
+  std::vector<int64_t> h_row_len;  // C blocks per row (host)
 };
 void free_symbolic(Ctx* ctx, Symbolic& s);
 
 int32_t check_compatible(Ctx* ctx, const DevMatrix* A, const DevMatrix* B);
-// Builds C's pattern (row_p, col, sector-major off, data buffer) and the stacks.
-int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, Symbolic* out);
-// Packs (data offset | k block size << 56) for every A block.
-int32_t pack_a_meta(Ctx* ctx, const DevMatrix* A, int64_t** a_offk);
-int32_t numeric_fp64(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, DevMatrix* C, const Symbolic& sym,
-                     const int64_t* a_offk, double* c_nrm);
-int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym,
-                      const int64_t* a_offk, double* c_nrm, int* slices_used);
+// Packs (data offset | column block size << 56) for every block of m.
+int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk);
+// Builds C's pattern (row_p, col, sector-major off, data buffer) and the
+// stacks; a_offk is required unless want_ids.
+int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, bool want_ids,
+                       const int64_t* a_offk, Symbolic* out);
+// Work list of C blocks in the row processing order of `order_src` (its h_order).
+int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
+                   int32_t** work_c);
+// Stacked small-GEMM kernels: out_c = sum_e op1_e . op2_e over the work list.
+// TA/TB select transposed operands (used by the adjoint); see numeric.cu.
+int32_t run_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
+                    const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2);
+int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,
+                      const int32_t* work_c, double* c_nrm, int* slices_used);
 // Drops C blocks with c_nrm < eps from the index (data stay in place).
 int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps, int64_t* dropped);
 // Full multiply on device handles (used by the C ABI, purification and batches).
 int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, uint32_t flags,
                       lamb_gpu_mult_stats* stats);
-
-constexpr int64_t kOffMask = (1ll << 56) - 1;
 
 }  // namespace lamb

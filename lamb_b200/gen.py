@@ -67,6 +67,14 @@ class WaterGeometry:
         lib.lamb_gen_geom_atoms(h, self.positions.ctypes.data, self.blk.ctypes.data, self.subset.ctypes.data,
                                 self.local.ctypes.data)
 
+    def sector_positions(self) -> np.ndarray:
+        """Atom coordinates in sector order (subset 1's atoms first, local order)."""
+        counts = np.bincount(self.subset, minlength=int(self.subset.max(initial=0)) + 1)[1:]
+        base = np.concatenate([[0], np.cumsum(counts)])
+        out = np.zeros((self.n_atoms, 3), np.float32)
+        out[base[self.subset - 1] + self.local] = self.positions
+        return out
+
     def matrix(self, seed: int, decay: float = 1.5, symmetric: bool = False, name: str = "matrix") -> LambMatrix:
         lib = _gen()
         m = C.c_void_p()
@@ -119,6 +127,8 @@ class WaterWorkload:
 WATER_192 = WaterWorkload("water192_cut6", 192, 17.9, 6.0, 1e-8, 0, 0, 0)
 # 6144 waters in a 56.8 A box, cutoff 8 A, A and B from seeds 1 and 2, eps 1e-10.
 WATER_6144 = WaterWorkload("water6144_cut8", 6144, 56.8, 8.0, 1e-10, 1, 1, 2)
+# 1536 waters at the same density, cutoff 7 A, seed 4 (the purification-adjoint geometry).
+WATER_1536 = WaterWorkload("water1536_cut7", 1536, box_side(1536), 7.0, 1e-10, 4, 4, 5)
 
 
 def batch_instances(n: int = 64, seed: int = 3, mol_range=(96, 1536), cut_range=(5.0, 9.0)):

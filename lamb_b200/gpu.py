@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
             "lamb_gpu_matrix_create_like": [vp, i64, P(i64)],
             "lamb_gpu_matrix_destroy": [vp, i64],
             "lamb_gpu_matrix_n_sectors": [vp, i64, P(i32)],
+            "lamb_gpu_matrix_set_positions": [vp, i64, vp, i32, vp],
             "lamb_gpu_matrix_query": [vp, i64, P(CSectorSizes), i32],
             "lamb_gpu_matrix_download": [vp, i64, P(CSectorOut), i32],
             "lamb_gpu_multiply": [vp, i64, i64, i64, dbl, u32, P(MultStats)],
@@ -200,6 +201,13 @@ class DeviceMatrix:
         arr = (CSectorOut * len(outs))(*outs)
         self.ctx.check(lib().lamb_gpu_matrix_download(self.ctx.handle, self.h, arr, len(outs)))
         return LambMatrix(secs, "C")
+
+    def set_positions(self, xyz: np.ndarray, box) -> None:
+        """Row-atom coordinates in sector order (locality hint for the multiply)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        bx = np.ascontiguousarray(np.broadcast_to(np.asarray(box, np.float32), (3,)))
+        self.ctx.check(lib().lamb_gpu_matrix_set_positions(self.ctx.handle, self.h, xyz.ctypes.data, xyz.shape[0],
+                                                           bx.ctypes.data))
 
     def destroy(self) -> None:
         if self.h:

@@ -179,3 +179,22 @@ def test_water6144_cut8_sampled_rows(gpu_ctx):
     den = sum(float(np.sum(ref[k] ** 2)) for k in ref)
     assert np.sqrt(num / den) <= TOL_FP64
     assert st["n_c_blocks"] == sum(s.n_blks for s in c.sectors)
+
+
+def test_positions_hint_does_not_change_results(gpu_ctx):
+    """The work order (Morton from coordinates vs Cuthill-McKee) leaves C bit-identical."""
+    g = WaterGeometry(96, None, 7.0, seed=12)
+    a, b = g.matrix(1), g.matrix(2)
+    outs = []
+    for use_pos in (False, True):
+        da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+        if use_pos:
+            da.set_positions(g.sector_positions(), g.box)
+        dc = gpu_ctx.create_like(da)
+        gpu_ctx.multiply(da, db, dc, 1e-10)
+        outs.append(dc.download())
+        for m in (dc, db, da):
+            m.destroy()
+    for s1, s2 in zip(outs[0].sectors, outs[1].sectors):
+        assert np.array_equal(s1.row_p, s2.row_p) and np.array_equal(s1.col_i, s2.col_i)
+        assert np.array_equal(s1.data, s2.data)
