@@ -455,7 +455,8 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
     if (flags & LAMB_GPU_MIXED)
       LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, &slices));
     else
-      LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false));
+      LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false,
+                              max_block(A->h_col_bs)));
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps, &dropped));
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));

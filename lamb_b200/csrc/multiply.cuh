@@ -53,8 +53,15 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
                    int32_t** work_c);
 // Stacked small-GEMM kernels: out_c = sum_e op1_e . op2_e over the work list.
 // TA/TB select transposed operands (used by the adjoint); see numeric.cu.
+// max_inner: the largest inner block size of any entry (sizes the column table).
 int32_t run_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
-                    const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2);
+                    const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2,
+                    int max_inner);
+inline int max_block(const std::vector<int8_t>& v) {
+  int m = 0;
+  for (int8_t x : v) m = x > m ? x : m;
+  return m;
+}
 int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,
                       const int32_t* work_c, double* c_nrm, int* slices_used);
 // Drops C blocks with c_nrm < eps from the index (data stay in place).

@@ -1,31 +1,35 @@
 // FP64 numeric phase: stacked small GEMMs on the FP64 tensor pipe (DMMA).
 //
 // This is the body of the reference's sector_multiply stub
-// (src/lamb_multiplication.F90:206-225): every C block is owned by one warp
-// (segment ownership, no atomics), which consumes the block's stack as ONE
-// concatenated inner dimension,
-//     C_ij = sum_e A_ik(e) . B_k(e)j = [A_ik1 | A_ik2 | ...] . [B_k1j ; B_k2j ; ...],
-// padded to a multiple of 4 once per 64 entries instead of once per entry.
-// The product runs as mma.m8n8k4.f64: MF x NF fragments of 8x8 cover the
-// M x N output block.  Fragment layouts (PTX ISA, mma.m8n8k4 with .f64):
-//   op1 (8x4, row): lane holds op1[lane/4][lane%4]
-//   op2 (4x8, col): lane holds op2[lane%4][lane/4]
-//   out (8x8):      lane holds out[lane/4][2*(lane%4) + {0,1}]
-// Operand fragments are loaded two windows (8 inner columns) ahead of the
-// mma that consumes them, and warps take work items in the row processing
-// order (Morton / Cuthill-McKee), so that the B rows of neighbouring C rows
-// stay resident in L2.
+// (src/lamb_multiplication.F90:206-225): every output block is owned by one
+// warp (segment ownership, no atomics), which consumes the block's stack as
+// ONE concatenated inner dimension,
+//     C_ij = sum_e op1_e . op2_e = [op1_1 | op1_2 | ...] . [op2_1 ; op2_2 ; ...],
+// padded once per chunk of entries instead of once per entry.
+//
+// Per chunk the warp writes a column table into shared memory: for every
+// inner column kk of the concatenated panel, the address of op1(0,kk) and
+// op2(kk,0) and their strides (so that op1(r,kk) = d1[a + r*sa] and
+// op2(kk,c) = d2[b + c*sb]).  One 16-byte shared load per column then serves
+// any operand transposition (forward product and both adjoint products).
+//
+// Products use mma.sync .f64 shapes (PTX ISA fragment layouts):
+//   m16n8k16 (blocks with 9..16 rows): op1 a_i at (g + 8*(i%2), t + 4*(i/2)),
+//     op2 b_i at (t + 4*i, g), out c_i at (g + 8*(i/2), 2t + i%2);
+//   m8n8k4 (blocks with <= 8 rows): op1 at (g, t), op2 at (t, g),
+//     out at (g, 2t + {0,1});
+// with g = lane/4, t = lane%4.  Both run on the FP64 tensor pipe at the same
+// peak; m16n8k16 does 16x the work per issued instruction.
 #include "multiply.cuh"
 
 namespace lamb {
 
 constexpr int kNumWarps = 8;
-constexpr int kChunk = 64;
+constexpr int kMaxChunk = 32;
 
-struct WarpBuf {
-  long long ao[kChunk];
-  long long bo[kChunk];
-  int pre[kChunk + 1];
+struct ColRef {
+  long long a;  // op1 column base | stride << 56
+  long long b;  // op2 row base | stride << 56
 };
 
 __device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
@@ -34,112 +38,158 @@ __device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double
                : "d"(a), "d"(b));
 }
 
-// Loads one chunk of <= 64 entries into the warp buffer; returns K (sum of
-// inner sizes).  Entries beyond m contribute nothing.
-__device__ __forceinline__ int load_chunk(const Ent* __restrict__ ent, int64_t first, int m, WarpBuf& wb,
-                                          int lane) {
-  Ent x0{0, 0}, x1{0, 0};
-  if (lane < m) x0 = ent[first + lane];
-  if (lane + 32 < m) x1 = ent[first + lane + 32];
-  const int k0 = lane < m ? (int)((unsigned long long)x0.a >> 56) : 0;
-  const int k1 = lane + 32 < m ? (int)((unsigned long long)x1.a >> 56) : 0;
-  const int i0 = warp_incl_scan(k0, lane);
-  const int t0 = __shfl_sync(0xffffffffu, i0, 31);
-  const int i1 = warp_incl_scan(k1, lane) + t0;
-  wb.ao[lane] = x0.a & kOffMask;
-  wb.bo[lane] = x0.b;
-  wb.ao[lane + 32] = x1.a & kOffMask;
-  wb.bo[lane + 32] = x1.b;
-  wb.pre[lane] = i0 - k0;
-  wb.pre[lane + 32] = i1 - k1;
-  if (lane == 31) wb.pre[kChunk] = i1;
-  __syncwarp();
-  return wb.pre[kChunk];
+__device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-template <int MF, int NF, bool TA, bool TB>
-struct Window {
-  double a[MF], b[NF];
-  __device__ __forceinline__ void load(const double* __restrict__ d1, const double* __restrict__ d2,
-                                       const WarpBuf& wb, int m, int K, int M, int N, int kw, int g, int t, int& e) {
-    const int colk = kw + t;
-    while (e < m - 1 && colk >= wb.pre[e + 1]) ++e;
-    const bool valid = colk < K;
-    const int kc = colk - wb.pre[e];
-    const int ke = wb.pre[e + 1] - wb.pre[e];
-    const double* p1 = d1 + wb.ao[e];
-    const double* p2 = d2 + wb.bo[e];
-#pragma unroll
-    for (int i = 0; i < MF; ++i) {
-      const int r = i * 8 + g;
-      a[i] = (valid && r < M) ? __ldg(p1 + (TA ? (int64_t)kc + (int64_t)r * ke : (int64_t)r + (int64_t)kc * M)) : 0.0;
-    }
-#pragma unroll
-    for (int j = 0; j < NF; ++j) {
-      const int cc = j * 8 + g;
-      b[j] = (valid && cc < N) ? __ldg(p2 + (TB ? (int64_t)cc + (int64_t)kc * N : (int64_t)kc + (int64_t)cc * ke)) : 0.0;
-    }
+// Loads up to `cap` entries starting at `first` and writes the column table;
+// returns K, the number of inner columns.  TA/TB: op1/op2 stored transposed.
+template <bool TA, bool TB>
+__device__ __forceinline__ int build_table(const Ent* __restrict__ ent, int64_t first, int m, int M, int N,
+                                           ColRef* __restrict__ tbl, int lane) {
+  Ent x{0, 0};
+  if (lane < m) x = ent[first + lane];
+  const int ke = lane < m ? (int)((unsigned long long)x.a >> 56) : 0;
+  const int incl = warp_incl_scan(ke, lane);
+  const int K = __shfl_sync(0xffffffffu, incl, 31);
+  const long long ao = x.a & kOffMask, bo = x.b;
+  const long long sa = TA ? ke : 1, sb = TB ? 1 : ke;
+  for (int kc = 0, kk = incl - ke; kc < ke; ++kc, ++kk) {
+    const long long ca = TA ? ao + kc : ao + (long long)kc * M;
+    const long long cb = TB ? bo + (long long)kc * N : bo + kc;
+    tbl[kk] = ColRef{ca | (sa << 56), cb | (sb << 56)};
   }
-};
+  __syncwarp();
+  return K;
+}
 
-template <int MF, int NF, bool TA, bool TB>
-__device__ __forceinline__ void stacked_block(const double* __restrict__ d1, const double* __restrict__ d2,
-                                              double* __restrict__ out, double* __restrict__ out_nrm, int64_t c,
-                                              int M, int N, int64_t o_off, int64_t s0, int n,
-                                              const Ent* __restrict__ ent, WarpBuf& wb) {
+__device__ __forceinline__ double ld_op(const double* __restrict__ d, long long ref, int idx, bool ok) {
+  return ok ? __ldg(d + ((ref & kOffMask) + (long long)idx * (ref >> 56))) : 0.0;
+}
+
+// Output rows r0 .. r0+15 of a block with more than 8 rows: m16n8k16.
+template <int NF, bool TA, bool TB>
+__device__ __forceinline__ void block_m16(const double* __restrict__ d1, const double* __restrict__ d2,
+                                          double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M,
+                                          int N, int r0, int64_t o_off, int64_t s0, int n,
+                                          const Ent* __restrict__ ent, ColRef* __restrict__ tbl, int cap) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
-  double acc[MF][NF][2];
+  double acc[NF][4];
 #pragma unroll
-  for (int i = 0; i < MF; ++i)
+  for (int j = 0; j < NF; ++j)
 #pragma unroll
-    for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  for (int base = 0; base < n; base += kChunk) {
-    const int m = min(kChunk, n - base);
-    const int K = load_chunk(ent, s0 + base, m, wb, lane);
-    int e = 0;
-    Window<MF, NF, TA, TB> w0, w1;
-    w0.load(d1, d2, wb, m, K, M, N, 0, g, t, e);
-    for (int kw = 0; kw < K; kw += 8) {
-      w1.load(d1, d2, wb, m, K, M, N, kw + 4, g, t, e);
+    for (int h = 0; h < 4; ++h) acc[j][h] = 0.0;
+  const int ra = r0 + g, rb = r0 + g + 8;
+  const bool rok0 = ra < M, rok1 = rb < M;
+  bool cok[NF];
 #pragma unroll
-      for (int i = 0; i < MF; ++i)
+  for (int j = 0; j < NF; ++j) cok[j] = j * 8 + g < N;
+  for (int base = 0; base < n; base += cap) {
+    const int m = min(cap, n - base);
+    const int K = build_table<TA, TB>(ent, s0 + base, m, M, N, tbl, lane);
+    for (int kw = 0; kw < K; kw += 16) {
+      double a[8], b[NF][4];
 #pragma unroll
-        for (int j = 0; j < NF; ++j) dmma884(acc[i][j][0], acc[i][j][1], w0.a[i], w0.b[j]);
-      w0.load(d1, d2, wb, m, K, M, N, kw + 8, g, t, e);
-      if (kw + 4 < K) {
+      for (int q = 0; q < 4; ++q) {
+        const int kk = kw + t + 4 * q;
+        const bool kv = kk < K;
+        const ColRef cr = tbl[kv ? kk : 0];
+        a[2 * q] = ld_op(d1, cr.a, ra, kv && rok0);
+        a[2 * q + 1] = ld_op(d1, cr.a, rb, kv && rok1);
 #pragma unroll
-        for (int i = 0; i < MF; ++i)
-#pragma unroll
-          for (int j = 0; j < NF; ++j) dmma884(acc[i][j][0], acc[i][j][1], w1.a[i], w1.b[j]);
+        for (int j = 0; j < NF; ++j) b[j][q] = ld_op(d2, cr.b, j * 8 + g, kv && cok[j]);
       }
+#pragma unroll
+      for (int j = 0; j < NF; ++j) dmma16816(acc[j], a, b[j]);
     }
     __syncwarp();
   }
   double sq = 0.0;
 #pragma unroll
-  for (int i = 0; i < MF; ++i)
+  for (int j = 0; j < NF; ++j)
 #pragma unroll
-    for (int j = 0; j < NF; ++j)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = i * 8 + g, cc = j * 8 + 2 * t + h;
-        if (r < M && cc < N) {
-          const double v = acc[i][j][h];
-          out[o_off + (int64_t)cc * M + r] = v;
-          sq = __fma_rn(v, v, sq);
-        }
+    for (int h = 0; h < 4; ++h) {
+      const int r = r0 + g + 8 * (h >> 1), cc = j * 8 + 2 * t + (h & 1);
+      if (r < M && cc < N) {
+        const double v = acc[j][h];
+        out[o_off + (int64_t)cc * M + r] = v;
+        sq = __fma_rn(v, v, sq);
       }
+    }
+  sq = warp_sum(sq);
+  if (out_nrm) {
+    // slabs of one block accumulate |C|^2 in order; the last slab takes the root
+    const double prev = (r0 == 0) ? 0.0 : out_nrm[c];
+    __syncwarp();
+    if (lane == 0) out_nrm[c] = (r0 + 16 >= M) ? __dsqrt_rn(prev + sq) : prev + sq;
+    __syncwarp();
+  }
+}
+
+// Output blocks with at most 8 rows: m8n8k4.
+template <int NF, bool TA, bool TB>
+__device__ __forceinline__ void block_m8(const double* __restrict__ d1, const double* __restrict__ d2,
+                                         double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M,
+                                         int N, int64_t o_off, int64_t s0, int n, const Ent* __restrict__ ent,
+                                         ColRef* __restrict__ tbl, int cap) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[NF][2];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) acc[j][0] = acc[j][1] = 0.0;
+  const bool rok = g < M;
+  bool cok[NF];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) cok[j] = j * 8 + g < N;
+  for (int base = 0; base < n; base += cap) {
+    const int m = min(cap, n - base);
+    const int K = build_table<TA, TB>(ent, s0 + base, m, M, N, tbl, lane);
+    for (int kw = 0; kw < K; kw += 8) {
+      double a[2], b[2][NF];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int kk = kw + 4 * u + t;
+        const bool kv = kk < K;
+        const ColRef cr = tbl[kv ? kk : 0];
+        a[u] = ld_op(d1, cr.a, g, kv && rok);
+#pragma unroll
+        for (int j = 0; j < NF; ++j) b[u][j] = ld_op(d2, cr.b, j * 8 + g, kv && cok[j]);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int j = 0; j < NF; ++j) dmma884(acc[j][0], acc[j][1], a[u], b[u][j]);
+    }
+    __syncwarp();
+  }
+  double sq = 0.0;
+#pragma unroll
+  for (int j = 0; j < NF; ++j)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cc = j * 8 + 2 * t + h;
+      if (g < M && cc < N) {
+        const double v = acc[j][h];
+        out[o_off + (int64_t)cc * M + g] = v;
+        sq = __fma_rn(v, v, sq);
+      }
+    }
   sq = warp_sum(sq);
   if (lane == 0 && out_nrm) out_nrm[c] = __dsqrt_rn(sq);
 }
 
-// Blocks larger than 24 in a dimension: plain FP64 FMAs, one output element
-// per lane and step.
+// Blocks larger than 32 rows or 24 columns: plain FP64 FMAs, one output
+// element per lane and step.
 template <bool TA, bool TB>
-__device__ void stacked_block_generic(const double* __restrict__ d1, const double* __restrict__ d2,
-                                      double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M,
-                                      int N, int64_t o_off, int64_t s0, int n, const Ent* __restrict__ ent) {
+__device__ void block_generic(const double* __restrict__ d1, const double* __restrict__ d2, double* __restrict__ out,
+                              double* __restrict__ out_nrm, int64_t c, int M, int N, int64_t o_off, int64_t s0, int n,
+                              const Ent* __restrict__ ent) {
   const int lane = threadIdx.x & 31;
   double sq = 0.0;
   for (int el = lane; el < M * N; el += 32) {
@@ -164,13 +214,13 @@ __device__ void stacked_block_generic(const double* __restrict__ d1, const doubl
 }
 
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(kNumWarps * 32, 3)
+__global__ void __launch_bounds__(kNumWarps * 32, 2)
     k_stacked(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
               const Ent* __restrict__ ent, const double* __restrict__ d1, const double* __restrict__ d2,
-              double* __restrict__ out, double* __restrict__ out_nrm) {
-  __shared__ WarpBuf wbs[kNumWarps];
+              double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_cols) {
+  extern __shared__ ColRef tbl_all[];
   const int w = threadIdx.x >> 5;
-  WarpBuf& wb = wbs[w];
+  ColRef* tbl = tbl_all + (size_t)w * tbl_cols;
   const int64_t nwarps = (int64_t)gridDim.x * kNumWarps;
   for (int64_t v = (int64_t)blockIdx.x * kNumWarps + w; v < n_work; v += nwarps) {
     const Work it = work[v];
@@ -179,45 +229,60 @@ __global__ void __launch_bounds__(kNumWarps * 32, 3)
     const int M = (int)((it.lo >> 40) & 0xff), N = (int)((it.lo >> 48) & 0xff);
     const int64_t s0 = it.hi & kMask40;
     const int n = (int)((unsigned long long)it.hi >> 40);
-    const int mf = (M + 7) >> 3, nf = (N + 7) >> 3;
-    if (mf == 0 || nf == 0) {
+    if (M == 0 || N == 0) {
       if ((threadIdx.x & 31) == 0 && out_nrm) out_nrm[c] = 0.0;
       continue;
     }
-    switch (mf * 4 + nf) {
-      case 1 * 4 + 1: stacked_block<1, 1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 1 * 4 + 2: stacked_block<1, 2, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 1 * 4 + 3: stacked_block<1, 3, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 2 * 4 + 1: stacked_block<2, 1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 2 * 4 + 2: stacked_block<2, 2, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 2 * 4 + 3: stacked_block<2, 3, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 3 * 4 + 1: stacked_block<3, 1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 3 * 4 + 2: stacked_block<3, 2, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      case 3 * 4 + 3: stacked_block<3, 3, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, wb); break;
-      default: stacked_block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent); break;
+    const int nf = (N + 7) >> 3;
+    if (M <= 8) {
+      switch (nf) {
+        case 1: block_m8<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap); break;
+        case 2: block_m8<2, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap); break;
+        case 3: block_m8<3, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap); break;
+        default: block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent); break;
+      }
+    } else if (nf <= 3) {
+      for (int r0 = 0; r0 < M; r0 += 16) {
+        switch (nf) {
+          case 1: block_m16<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+          case 2: block_m16<2, TA, TB>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+          default: block_m16<3, TA, TB>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+        }
+      }
+    } else {
+      block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent);
     }
   }
 }
 
 template <bool TA, bool TB>
 static int32_t launch_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
-                              const double* d1, const double* d2, double* out, double* out_nrm) {
+                              const double* d1, const double* d2, double* out, double* out_nrm, int max_inner) {
+  // Column table per warp: `cap` entries of up to max_inner columns each.
+  const int mi = std::max(1, std::min(max_inner, 127));
+  int cap = std::max(1, std::min(kMaxChunk, 8192 / mi));
+  const int tbl_cols = cap * mi;
+  const size_t smem = sizeof(ColRef) * (size_t)tbl_cols * kNumWarps;
+  auto kern = k_stacked<TA, TB>;
+  if (smem > 48 * 1024)
+    LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stacked<TA, TB>, kNumWarps * 32, 0));
+  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNumWarps * 32, smem));
   const int64_t need = (n_work + kNumWarps - 1) / kNumWarps;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * std::max(per_sm, 1)));
-  k_stacked<TA, TB><<<grid, kNumWarps * 32, 0, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm);
+  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols);
   LAMB_LAUNCHED(ctx);
   return LAMB_GPU_OK;
 }
 
 int32_t run_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
-                    const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2) {
+                    const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2,
+                    int max_inner) {
   if (n_work == 0) return LAMB_GPU_OK;
-  if (!t1 && !t2) return launch_stacked<false, false>(ctx, n_work, work, work_c, ent, d1, d2, out, out_nrm);
-  if (!t1 && t2) return launch_stacked<false, true>(ctx, n_work, work, work_c, ent, d1, d2, out, out_nrm);
-  if (t1 && !t2) return launch_stacked<true, false>(ctx, n_work, work, work_c, ent, d1, d2, out, out_nrm);
+  if (!t1 && !t2) return launch_stacked<false, false>(ctx, n_work, work, work_c, ent, d1, d2, out, out_nrm, max_inner);
+  if (!t1 && t2) return launch_stacked<false, true>(ctx, n_work, work, work_c, ent, d1, d2, out, out_nrm, max_inner);
+  if (t1 && !t2) return launch_stacked<true, false>(ctx, n_work, work, work_c, ent, d1, d2, out, out_nrm, max_inner);
   return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "unsupported operand transposition");
 }
 

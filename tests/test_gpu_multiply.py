@@ -198,3 +198,14 @@ def test_positions_hint_does_not_change_results(gpu_ctx):
     for s1, s2 in zip(outs[0].sectors, outs[1].sectors):
         assert np.array_equal(s1.row_p, s2.row_p) and np.array_equal(s1.col_i, s2.col_i)
         assert np.array_equal(s1.data, s2.data)
+
+
+@pytest.mark.parametrize("blk_o,blk_h", [(23, 5), (13, 5), (3, 1), (40, 7)])
+def test_block_size_classes(gpu_ctx, blk_o, blk_h):
+    """m8n8k4 (<= 8 rows), m16n8k16 slabs (9..32 rows) and the generic path (> 24 columns)."""
+    g = WaterGeometry(40, None, 6.0, blk_o=blk_o, blk_h=blk_h, seed=3)
+    a, b = g.matrix(1), g.matrix(2)
+    c_ref, _ = oracle.multiply(a, b, 0.0)
+    c, _ = _gpu_mult(gpu_ctx, a, b, 0.0)
+    assert_same_pattern(c, c_ref)
+    assert rel_frobenius_error(c, c_ref) <= TOL_FP64
