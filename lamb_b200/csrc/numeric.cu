@@ -27,9 +27,11 @@ namespace lamb {
 constexpr int kNumWarps = 8;
 constexpr int kMaxChunk = 32;
 
+// Column table entry: pointers to op1(0,kk) and op2(kk,0); the runtime
+// stride (the entry's inner block size) sits in the top byte of `pbk`.
 struct ColRef {
-  long long a;  // op1 column base | stride << 56
-  long long b;  // op2 row base | stride << 56
+  const double* pa;
+  unsigned long long pbk;
 };
 
 __device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
@@ -48,51 +50,67 @@ __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], 
 }
 
 // Loads up to `cap` entries starting at `first` and writes the column table;
-// returns K, the number of inner columns.  TA/TB: op1/op2 stored transposed.
+// returns K, the number of inner columns.  TA/TB: op1/op2 stored transposed,
+// i.e. op1(r,kk) = pa[r*ke] (else pa[r]) and op2(kk,c) = pb[c] (else pb[c*ke]).
 template <bool TA, bool TB>
-__device__ __forceinline__ int build_table(const Ent* __restrict__ ent, int64_t first, int m, int M, int N,
+__device__ __forceinline__ int build_table(const double* __restrict__ d1, const double* __restrict__ d2,
+                                           const Ent* __restrict__ ent, int64_t first, int m, int M, int N,
                                            ColRef* __restrict__ tbl, int lane) {
   Ent x{0, 0};
   if (lane < m) x = ent[first + lane];
   const int ke = lane < m ? (int)((unsigned long long)x.a >> 56) : 0;
   const int incl = warp_incl_scan(ke, lane);
   const int K = __shfl_sync(0xffffffffu, incl, 31);
-  const long long ao = x.a & kOffMask, bo = x.b;
-  const long long sa = TA ? ke : 1, sb = TB ? 1 : ke;
+  const double* pa = d1 + (x.a & kOffMask);
+  const double* pb = d2 + x.b;
+  const unsigned long long kb = (unsigned long long)ke << 56;
   for (int kc = 0, kk = incl - ke; kc < ke; ++kc, ++kk) {
-    const long long ca = TA ? ao + kc : ao + (long long)kc * M;
-    const long long cb = TB ? bo + (long long)kc * N : bo + kc;
-    tbl[kk] = ColRef{ca | (sa << 56), cb | (sb << 56)};
+    const double* ca = TA ? pa + kc : pa + (int64_t)kc * M;
+    const double* cb = TB ? pb + (int64_t)kc * N : pb + kc;
+    tbl[kk] = ColRef{ca, (unsigned long long)cb | kb};
   }
   __syncwarp();
   return K;
 }
 
-__device__ __forceinline__ double ld_op(const double* __restrict__ d, long long ref, int idx, bool ok) {
-  return ok ? __ldg(d + ((ref & kOffMask) + (long long)idx * (ref >> 56))) : 0.0;
+// op1(r, kk) and op2(kk, c) for one table column.
+template <bool TA>
+__device__ __forceinline__ double ld1(const ColRef& cr, int r, int ke, bool ok) {
+  return ok ? __ldg(cr.pa + (TA ? (int64_t)r * ke : (int64_t)r)) : 0.0;
 }
+template <bool TB>
+__device__ __forceinline__ double ld2(const double* pb, int c, int ke, bool ok) {
+  return ok ? __ldg(pb + (TB ? (int64_t)c : (int64_t)c * ke)) : 0.0;
+}
+__device__ __forceinline__ const double* col_pb(const ColRef& cr) {
+  return reinterpret_cast<const double*>(cr.pbk & kOffMask);
+}
+__device__ __forceinline__ int col_ke(const ColRef& cr) { return (int)(cr.pbk >> 56); }
 
-// Output rows r0 .. r0+15 of a block with more than 8 rows: m16n8k16.
-template <int NF, bool TA, bool TB>
+// m16n8k16 on 16 output rows r0..r0+15 of a block with more than 8 rows.
+// SWAP computes the transposed block (used when the block has <= 8 rows but
+// more than 8 columns): tile rows are the block's columns.
+template <int NF, bool TA, bool TB, bool SWAP>
 __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const double* __restrict__ d2,
                                           double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M,
                                           int N, int r0, int64_t o_off, int64_t s0, int n,
                                           const Ent* __restrict__ ent, ColRef* __restrict__ tbl, int cap) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
+  const int TM = SWAP ? N : M, TN = SWAP ? M : N;  // tile rows / columns
   double acc[NF][4];
 #pragma unroll
   for (int j = 0; j < NF; ++j)
 #pragma unroll
     for (int h = 0; h < 4; ++h) acc[j][h] = 0.0;
   const int ra = r0 + g, rb = r0 + g + 8;
-  const bool rok0 = ra < M, rok1 = rb < M;
+  const bool rok0 = ra < TM, rok1 = rb < TM;
   bool cok[NF];
 #pragma unroll
-  for (int j = 0; j < NF; ++j) cok[j] = j * 8 + g < N;
+  for (int j = 0; j < NF; ++j) cok[j] = j * 8 + g < TN;
   for (int base = 0; base < n; base += cap) {
     const int m = min(cap, n - base);
-    const int K = build_table<TA, TB>(ent, s0 + base, m, M, N, tbl, lane);
+    const int K = build_table<TA, TB>(d1, d2, ent, s0 + base, m, M, N, tbl, lane);
     for (int kw = 0; kw < K; kw += 16) {
       double a[8], b[NF][4];
 #pragma unroll
@@ -100,10 +118,20 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
         const int kk = kw + t + 4 * q;
         const bool kv = kk < K;
         const ColRef cr = tbl[kv ? kk : 0];
-        a[2 * q] = ld_op(d1, cr.a, ra, kv && rok0);
-        a[2 * q + 1] = ld_op(d1, cr.a, rb, kv && rok1);
+        const int ke = col_ke(cr);
+        const double* pb = col_pb(cr);
+        if (!SWAP) {
+          a[2 * q] = ld1<TA>(cr, ra, ke, kv && rok0);
+          a[2 * q + 1] = ld1<TA>(cr, rb, ke, kv && rok1);
 #pragma unroll
-        for (int j = 0; j < NF; ++j) b[j][q] = ld_op(d2, cr.b, j * 8 + g, kv && cok[j]);
+          for (int j = 0; j < NF; ++j) b[j][q] = ld2<TB>(pb, j * 8 + g, ke, kv && cok[j]);
+        } else {
+          // tile op1(r', kk) = op2(kk, r'); tile op2(kk, c') = op1(c', kk)
+          a[2 * q] = ld2<TB>(pb, ra, ke, kv && rok0);
+          a[2 * q + 1] = ld2<TB>(pb, rb, ke, kv && rok1);
+#pragma unroll
+          for (int j = 0; j < NF; ++j) b[j][q] = ld1<TA>(cr, j * 8 + g, ke, kv && cok[j]);
+        }
       }
 #pragma unroll
       for (int j = 0; j < NF; ++j) dmma16816(acc[j], a, b[j]);
@@ -116,9 +144,12 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
       const int r = r0 + g + 8 * (h >> 1), cc = j * 8 + 2 * t + (h & 1);
-      if (r < M && cc < N) {
+      if (r < TM && cc < TN) {
         const double v = acc[j][h];
-        out[o_off + (int64_t)cc * M + r] = v;
+        if (SWAP)
+          out[o_off + (int64_t)r * M + cc] = v;
+        else
+          out[o_off + (int64_t)cc * M + r] = v;
         sq = __fma_rn(v, v, sq);
       }
     }
@@ -127,7 +158,7 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
     // slabs of one block accumulate |C|^2 in order; the last slab takes the root
     const double prev = (r0 == 0) ? 0.0 : out_nrm[c];
     __syncwarp();
-    if (lane == 0) out_nrm[c] = (r0 + 16 >= M) ? __dsqrt_rn(prev + sq) : prev + sq;
+    if (lane == 0) out_nrm[c] = (r0 + 16 >= TM) ? __dsqrt_rn(prev + sq) : prev + sq;
     __syncwarp();
   }
 }
@@ -149,7 +180,7 @@ __device__ __forceinline__ void block_m8(const double* __restrict__ d1, const do
   for (int j = 0; j < NF; ++j) cok[j] = j * 8 + g < N;
   for (int base = 0; base < n; base += cap) {
     const int m = min(cap, n - base);
-    const int K = build_table<TA, TB>(ent, s0 + base, m, M, N, tbl, lane);
+    const int K = build_table<TA, TB>(d1, d2, ent, s0 + base, m, M, N, tbl, lane);
     for (int kw = 0; kw < K; kw += 8) {
       double a[2], b[2][NF];
 #pragma unroll
@@ -157,9 +188,11 @@ __device__ __forceinline__ void block_m8(const double* __restrict__ d1, const do
         const int kk = kw + 4 * u + t;
         const bool kv = kk < K;
         const ColRef cr = tbl[kv ? kk : 0];
-        a[u] = ld_op(d1, cr.a, g, kv && rok);
+        const int ke = col_ke(cr);
+        const double* pb = col_pb(cr);
+        a[u] = ld1<TA>(cr, g, ke, kv && rok);
 #pragma unroll
-        for (int j = 0; j < NF; ++j) b[u][j] = ld_op(d2, cr.b, j * 8 + g, kv && cok[j]);
+        for (int j = 0; j < NF; ++j) b[u][j] = ld2<TB>(pb, j * 8 + g, ke, kv && cok[j]);
       }
 #pragma unroll
       for (int u = 0; u < 2; ++u)
@@ -234,19 +267,17 @@ __global__ void __launch_bounds__(kNumWarps * 32, 2)
       continue;
     }
     const int nf = (N + 7) >> 3;
-    if (M <= 8) {
-      switch (nf) {
-        case 1: block_m8<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap); break;
-        case 2: block_m8<2, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap); break;
-        case 3: block_m8<3, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap); break;
-        default: block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent); break;
-      }
-    } else if (nf <= 3) {
+    if (M <= 8 && N <= 8) {
+      block_m8<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap);
+    } else if (M <= 8 && N <= 32) {
+      for (int r0 = 0; r0 < N; r0 += 16)
+        block_m16<1, TA, TB, true>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap);
+    } else if (M <= 32 && nf <= 3) {
       for (int r0 = 0; r0 < M; r0 += 16) {
         switch (nf) {
-          case 1: block_m16<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
-          case 2: block_m16<2, TA, TB>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
-          default: block_m16<3, TA, TB>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+          case 1: block_m16<1, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+          case 2: block_m16<2, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+          default: block_m16<3, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
         }
       }
     } else {
