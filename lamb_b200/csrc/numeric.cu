@@ -93,8 +93,9 @@ __device__ __forceinline__ int col_ke(const ColRef& cr) { return (int)(cr.pbk >>
 template <int NF, bool TA, bool TB, bool SWAP>
 __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const double* __restrict__ d2,
                                           double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M,
-                                          int N, int r0, int64_t o_off, int64_t s0, int n,
-                                          const Ent* __restrict__ ent, ColRef* __restrict__ tbl, int cap) {
+                                          int N, int r0, int c0, int64_t o_off, int64_t s0, int n,
+                                          const Ent* __restrict__ ent, ColRef* __restrict__ tbl, int cap,
+                                          bool last_slab) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   const int TM = SWAP ? N : M, TN = SWAP ? M : N;  // tile rows / columns
@@ -107,7 +108,7 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
   const bool rok0 = ra < TM, rok1 = rb < TM;
   bool cok[NF];
 #pragma unroll
-  for (int j = 0; j < NF; ++j) cok[j] = j * 8 + g < TN;
+  for (int j = 0; j < NF; ++j) cok[j] = c0 + j * 8 + g < TN;
   for (int base = 0; base < n; base += cap) {
     const int m = min(cap, n - base);
     const int K = build_table<TA, TB>(d1, d2, ent, s0 + base, m, M, N, tbl, lane);
@@ -124,13 +125,13 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
           a[2 * q] = ld1<TA>(cr, ra, ke, kv && rok0);
           a[2 * q + 1] = ld1<TA>(cr, rb, ke, kv && rok1);
 #pragma unroll
-          for (int j = 0; j < NF; ++j) b[j][q] = ld2<TB>(pb, j * 8 + g, ke, kv && cok[j]);
+          for (int j = 0; j < NF; ++j) b[j][q] = ld2<TB>(pb, c0 + j * 8 + g, ke, kv && cok[j]);
         } else {
           // tile op1(r', kk) = op2(kk, r'); tile op2(kk, c') = op1(c', kk)
           a[2 * q] = ld2<TB>(pb, ra, ke, kv && rok0);
           a[2 * q + 1] = ld2<TB>(pb, rb, ke, kv && rok1);
 #pragma unroll
-          for (int j = 0; j < NF; ++j) b[j][q] = ld1<TA>(cr, j * 8 + g, ke, kv && cok[j]);
+          for (int j = 0; j < NF; ++j) b[j][q] = ld1<TA>(cr, c0 + j * 8 + g, ke, kv && cok[j]);
         }
       }
 #pragma unroll
@@ -143,7 +144,7 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
   for (int j = 0; j < NF; ++j)
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
-      const int r = r0 + g + 8 * (h >> 1), cc = j * 8 + 2 * t + (h & 1);
+      const int r = r0 + g + 8 * (h >> 1), cc = c0 + j * 8 + 2 * t + (h & 1);
       if (r < TM && cc < TN) {
         const double v = acc[j][h];
         if (SWAP)
@@ -156,9 +157,9 @@ __device__ __forceinline__ void block_m16(const double* __restrict__ d1, const d
   sq = warp_sum(sq);
   if (out_nrm) {
     // slabs of one block accumulate |C|^2 in order; the last slab takes the root
-    const double prev = (r0 == 0) ? 0.0 : out_nrm[c];
+    const double prev = (r0 == 0 && c0 == 0) ? 0.0 : out_nrm[c];
     __syncwarp();
-    if (lane == 0) out_nrm[c] = (r0 + 16 >= TM) ? __dsqrt_rn(prev + sq) : prev + sq;
+    if (lane == 0) out_nrm[c] = last_slab ? __dsqrt_rn(prev + sq) : prev + sq;
     __syncwarp();
   }
 }
@@ -247,7 +248,7 @@ __device__ void block_generic(const double* __restrict__ d1, const double* __res
 }
 
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(kNumWarps * 32, 2)
+__global__ void __launch_bounds__(kNumWarps * 32, 3)
     k_stacked(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
               const Ent* __restrict__ ent, const double* __restrict__ d1, const double* __restrict__ d2,
               double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_cols) {
@@ -271,15 +272,17 @@ __global__ void __launch_bounds__(kNumWarps * 32, 2)
       block_m8<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap);
     } else if (M <= 8 && N <= 32) {
       for (int r0 = 0; r0 < N; r0 += 16)
-        block_m16<1, TA, TB, true>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap);
-    } else if (M <= 32 && nf <= 3) {
-      for (int r0 = 0; r0 < M; r0 += 16) {
-        switch (nf) {
-          case 1: block_m16<1, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
-          case 2: block_m16<2, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
-          default: block_m16<3, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, o_off, s0, n, ent, tbl, cap); break;
+        block_m16<1, TA, TB, true>(d1, d2, out, out_nrm, c, M, N, r0, 0, o_off, s0, n, ent, tbl, cap, r0 + 16 >= N);
+    } else if (M <= 32 && N <= 32) {
+      // 16-row x 16-column slabs (the last may be 8 columns wide)
+      for (int r0 = 0; r0 < M; r0 += 16)
+        for (int c0 = 0; c0 < N; c0 += 16) {
+          const bool last = r0 + 16 >= M && c0 + 16 >= N;
+          if (N - c0 > 8)
+            block_m16<2, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
+          else
+            block_m16<1, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
         }
-      }
     } else {
       block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent);
     }
