@@ -8,17 +8,6 @@ using namespace lamb;
   return fail(reinterpret_cast<Ctx*>(ctxp), LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "not built yet")
 
 extern "C" {
-int32_t lamb_gpu_matrix_axpby(lamb_gpu_ctx* c, double, lamb_gpu_matrix, double, lamb_gpu_matrix) { LAMB_PENDING(c); }
-int32_t lamb_gpu_matrix_copy(lamb_gpu_ctx* c, lamb_gpu_matrix, lamb_gpu_matrix) { LAMB_PENDING(c); }
-int32_t lamb_gpu_matrix_trace(lamb_gpu_ctx* c, lamb_gpu_matrix, double*) { LAMB_PENDING(c); }
-int32_t lamb_gpu_matrix_trace_product(lamb_gpu_ctx* c, lamb_gpu_matrix, lamb_gpu_matrix, double*) { LAMB_PENDING(c); }
-int32_t lamb_gpu_matrix_frobenius(lamb_gpu_ctx* c, lamb_gpu_matrix, double*) { LAMB_PENDING(c); }
-int32_t lamb_gpu_matrix_diff_frobenius(lamb_gpu_ctx* c, lamb_gpu_matrix, lamb_gpu_matrix, double*) { LAMB_PENDING(c); }
-int32_t lamb_gpu_matrix_scale_shift(lamb_gpu_ctx* c, lamb_gpu_matrix, double, double) { LAMB_PENDING(c); }
-int32_t lamb_gpu_purify_mcweeny(lamb_gpu_ctx* c, lamb_gpu_matrix, double, int32_t, int32_t, double, lamb_gpu_matrix,
-                                lamb_gpu_purify_report*) { LAMB_PENDING(c); }
-int32_t lamb_gpu_multiply_adjoint(lamb_gpu_ctx* c, lamb_gpu_matrix, lamb_gpu_matrix, lamb_gpu_matrix, lamb_gpu_matrix,
-                                  lamb_gpu_matrix) { LAMB_PENDING(c); }
 int32_t lamb_gpu_batch_create(lamb_gpu_ctx* c, const lamb_gpu_matrix*, const lamb_gpu_matrix*, const lamb_gpu_matrix*,
                               int32_t, double, lamb_gpu_batch**) { LAMB_PENDING(c); }
 int32_t lamb_gpu_batch_execute(lamb_gpu_batch*, lamb_gpu_mult_stats*) {

@@ -182,3 +182,45 @@ def random_fill_matrix(seed: int, n_atoms: Optional[int] = None, max_atoms: int 
             secs.append(Sector(m + 1, n + 1, rbs, cbs, row_p, (cols + 1).astype(np.int16),
                                np.stack([starts + 1, ends], axis=1).astype(np.int64).reshape(-1, 2), data))
     return LambMatrix(secs, name)
+
+
+def gapped_hamiltonian(geom: "WaterGeometry", seed: int, gap: float = 0.2, occ_fraction: float = 0.3,
+                       decay: float = 1.5) -> LambMatrix:
+    """Symmetric block-sparse H on the geometry's pattern with a spectral gap
+    of at least `gap` around mu = 0.
+
+    H = V + D: V is the symmetric water matrix (entries u*exp(-r/decay),
+    diagonal blocks (X+X^T)/2 + I); D is diagonal with d_p = -(gap/2 + R_p)
+    for the first round(occ_fraction*b) functions of every atom (occupied)
+    and +(gap/2 + R_p) for the rest, R_p = sum_q |V_pq| (row p of V).  Every
+    Gershgorin disc of H then lies outside (-gap/2, gap/2)."""
+    v = geom.matrix(seed, decay, symmetric=True, name="H")
+    # row sums of |V| per element row, per subset
+    sub_sizes = v.subset_blk_sizes(0)
+    offs = [np.concatenate([[0], np.cumsum(b.astype(np.int64))]) for b in sub_sizes]
+    rsum = [np.zeros(int(o[-1])) for o in offs]
+    for s in v.sectors:
+        rows = s.block_rows()
+        for blk in range(s.n_blks):
+            r, c = int(rows[blk]), int(s.col_i[blk]) - 1
+            m, n = int(s.row_blk_sizes[r]), int(s.col_blk_sizes[c])
+            f = int(s.extents[blk, 0])
+            x = s.data[f - 1:f - 1 + m * n].reshape(n, m).T
+            rsum[s.subset_row - 1][offs[s.subset_row - 1][r]:offs[s.subset_row - 1][r] + m] += np.abs(x).sum(axis=1)
+    for s in v.sectors:
+        if s.subset_row != s.subset_col:
+            continue
+        rows = s.block_rows()
+        o = offs[s.subset_row - 1]
+        rs = rsum[s.subset_row - 1]
+        for blk in range(s.n_blks):
+            r, c = int(rows[blk]), int(s.col_i[blk]) - 1
+            if r != c:
+                continue
+            m = int(s.row_blk_sizes[r])
+            f = int(s.extents[blk, 0])
+            n_occ = int(round(occ_fraction * m))
+            for p in range(m):
+                sign = -1.0 if p < n_occ else 1.0
+                s.data[f - 1 + p * m + p] += sign * (0.5 * gap + rs[o[r] + p])
+    return v

@@ -147,6 +147,46 @@ class Context:
         self.check(lib().lamb_gpu_multiply(self._h, a.h, b.h, c.h, eps, flags, C.byref(st)))
         return st.as_dict()
 
+    # -- algebra ------------------------------------------------------------------
+    def axpby(self, alpha: float, x: "DeviceMatrix", beta: float, y: "DeviceMatrix") -> None:
+        """y := alpha*x + beta*y over the union pattern."""
+        self.check(lib().lamb_gpu_matrix_axpby(self._h, alpha, x.h, beta, y.h))
+
+    def copy(self, x: "DeviceMatrix", y: "DeviceMatrix") -> None:
+        self.check(lib().lamb_gpu_matrix_copy(self._h, x.h, y.h))
+
+    def scale_shift(self, x: "DeviceMatrix", alpha: float, shift: float = 0.0) -> None:
+        self.check(lib().lamb_gpu_matrix_scale_shift(self._h, x.h, alpha, shift))
+
+    def _scalar(self, fn, *hs) -> float:
+        v = C.c_double()
+        self.check(fn(self._h, *[m.h for m in hs], C.byref(v)))
+        return v.value
+
+    def trace(self, x: "DeviceMatrix") -> float:
+        return self._scalar(lib().lamb_gpu_matrix_trace, x)
+
+    def trace_product(self, x: "DeviceMatrix", y: "DeviceMatrix") -> float:
+        return self._scalar(lib().lamb_gpu_matrix_trace_product, x, y)
+
+    def frobenius(self, x: "DeviceMatrix") -> float:
+        return self._scalar(lib().lamb_gpu_matrix_frobenius, x)
+
+    def diff_frobenius(self, x: "DeviceMatrix", y: "DeviceMatrix") -> float:
+        return self._scalar(lib().lamb_gpu_matrix_diff_frobenius, x, y)
+
+    def purify(self, h: "DeviceMatrix", p: "DeviceMatrix", mu: float = 0.0, steps: int = 30, fp64_tail: int = 5,
+               eps: float = 0.0) -> dict:
+        """McWeeny purification of h into p (p from create_like(h))."""
+        rep = PurifyReport()
+        self.check(lib().lamb_gpu_purify_mcweeny(self._h, h.h, mu, steps, fp64_tail, eps, p.h, C.byref(rep)))
+        return {k: getattr(rep, k) for k, _ in rep._fields_}
+
+    def adjoint(self, a: "DeviceMatrix", b: "DeviceMatrix", dc: "DeviceMatrix", da: Optional["DeviceMatrix"],
+                db: Optional["DeviceMatrix"]) -> None:
+        """da := (dc . b^T) on a's pattern, db := (a^T . dc) on b's pattern."""
+        self.check(lib().lamb_gpu_multiply_adjoint(self._h, a.h, b.h, dc.h, da.h if da else 0, db.h if db else 0))
+
     def stacks(self, a: "DeviceMatrix", b: "DeviceMatrix", c: "DeviceMatrix", eps: float = 0.0,
                flags: int = 0) -> np.ndarray:
         n = C.c_int64(0)
