@@ -254,6 +254,44 @@ LAMB_API int32_t lamb_gpu_batch_create(lamb_gpu_ctx* ctx, const lamb_gpu_matrix*
 LAMB_API int32_t lamb_gpu_batch_execute(lamb_gpu_batch* batch, lamb_gpu_mult_stats* stats);
 LAMB_API int32_t lamb_gpu_batch_destroy(lamb_gpu_batch* batch);
 
+/* ---- allocation-free entry point ------------------------------------------ */
+/* A block-CSR matrix already resident on the device, in the global sector
+ * order described above (all pointers are device addresses): row r's blocks
+ * are row_p[r] .. row_p[r+1]-1 with global columns col[] ascending, block b
+ * is row_bs[r] x col_bs[col[b]] column-major at data + off[b]. */
+typedef struct lamb_gpu_dcsr {
+  int32_t n_rows, n_cols;
+  int64_t nnz;
+  const int8_t* row_bs;
+  const int8_t* col_bs;
+  const int64_t* row_p;
+  const int32_t* col;
+  const int64_t* off;
+  const double* data;
+} lamb_gpu_dcsr;
+
+#define LAMB_GPU_NOALLOC_MAX_BLOCKS (1 << 20)
+
+/* Tr(X.Y) for callers that must not allocate device memory (no counterpart in
+ * the reference).  Some hosts cannot let a library call cudaMalloc: a code
+ * that has handed the whole GPU to its own memory pool at start-up (as
+ * Fortran electronic-structure codes often do, so a late cudaMalloc fails or
+ * fragments that pool), or one that runs this call between its own
+ * pre-allocated stages where an allocation would synchronise the device and
+ * break its timing.  This variant takes X and Y as caller-owned device
+ * arrays, returns the trace in *result (host memory) and keeps its working
+ * storage in a fixed array inside the library: 8 MiB of device memory per
+ * GPU, held from the library's first use on that GPU until the process
+ * exits.  X may hold at most LAMB_GPU_NOALLOC_MAX_BLOCKS blocks; larger X is
+ * rejected with a lamb_wrong_args status.  The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  Every call uses
+ * the same array, so calls whose work overlaps on the GPU (other streams or
+ * threads) race with each other; serialise them.  Runs on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) and synchronises it. */
+LAMB_API int32_t lamb_gpu_trace_product_noalloc(const lamb_gpu_dcsr* x, const lamb_gpu_dcsr* y, void* stream,
+                                                double* result);
+
 #ifdef __cplusplus
 }
 #endif
