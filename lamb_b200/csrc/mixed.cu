@@ -1,12 +1,394 @@
-// Mixed-precision numeric phase (int8 split slices on the tensor cores).
+// Mixed-precision numeric phase: FP64 block products as exact int8 slice
+// products on the tensor cores with FP64 recombination (the split-and-sum
+// scheme of Ozaki, Ogita, Oishi and Rump, Numer. Algorithms 59 (2012), with
+// int8 digits).  No reference counterpart.
+//
+// Every element row r of A gets a power-of-two scale 2^ea_r >= max_k |A(r,k)|
+// and every element column c of B a scale 2^eb_c >= max_k |B(k,c)|.  A scaled
+// value x in [-1, 1] is written as x = sum_p d_p w_p + rest with integer
+// digits d_p in [-64, 64], w_1 = 2^-6 and w_p = 2^-6-7(p-1) (each digit takes
+// the next 7 bits; |rest| <= w_s / 2).  Then
+//   C(r,c) = 2^(ea_r + eb_c) * sum_{p+q <= s+1} w_p w_q (D_p . E_q)(r,c),
+// where D_p, E_q are the digit planes of A and B.  Each plane product is an
+// exact int32 sum (|d| <= 64, so 2^19 inner terms fit) computed with
+// mma.m16n8k32 .s8.s8.s32; the recombination runs in FP64.  Pairs with
+// p + q > s+1 are dropped: their weight is below 2^-(12+7s).
+//
+// Plane layout: A block (M x ke) as M rows of pad4(ke) int8 (row-major), B
+// block (ke x N) as N columns of pad4(ke) int8, so that every 32-bit word is
+// four consecutive inner indices of one row (A) or one column (B) -- the
+// operand words of the m16n8k32 fragments:
+//   op1 a0,a1,a2,a3 = words (g, t), (g+8, t), (g, 4+t), (g+8, 4+t)
+//   op2 b0,b1       = words (col g, t), (col g, 4+t)
+//   out c0..c3      = (g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1)
+// with g = lane/4, t = lane%4 (PTX ISA fragment layout of mma.m16n8k32 for
+// 8-bit integer types).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+
+#include "algebra.cuh"
 #include "multiply.cuh"
 
 namespace lamb {
 
-int32_t numeric_mixed(Ctx* ctx, DevMatrix*, DevMatrix*, DevMatrix*, const Symbolic&, const Work*, const int32_t*,
-                      double*, int* slices_used) {
-  *slices_used = 0;
-  return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "mixed precision not built yet");
+constexpr int kMixWarps = 4;
+constexpr int kMaxSlices = 8;
+
+__device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
+
+// ---- scales ----------------------------------------------------------------------------
+// Row exponents of A: one warp per block row, one lane per element row.
+__global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                          const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                          const int8_t* __restrict__ col_bs, const double* __restrict__ d,
+                          const int64_t* __restrict__ ebase, int* __restrict__ ea) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
+    const int bi = row_bs[r];
+    for (int p = lane; p < bi; p += 32) {
+      double m = 0.0;
+      for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+        const int bk = col_bs[col[b]];
+        const double* x = d + off[b];
+        for (int q = 0; q < bk; ++q) m = fmax(m, fabs(x[(int64_t)q * bi + p]));
+      }
+      int e = 0;
+      frexp(m, &e);
+      ea[ebase[r] + p] = e;
+    }
+  }
+}
+
+// Column exponents of B: one thread per block, atomic max per element column.
+__global__ void k_col_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                          const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                          const int8_t* __restrict__ col_bs, const double* __restrict__ d,
+                          const int64_t* __restrict__ ebase, int* __restrict__ eb) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int bk = row_bs[r];
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      const int j = col[b], bj = col_bs[j];
+      const double* x = d + off[b];
+      for (int c = 0; c < bj; ++c) {
+        double m = 0.0;
+        for (int kk = 0; kk < bk; ++kk) m = fmax(m, fabs(x[(int64_t)c * bk + kk]));
+        int e = 0;
+        frexp(m, &e);
+        atomicMax(&eb[ebase[j] + c], e);
+      }
+    }
+  }
+}
+
+// Plane block sizes: A block (M x ke) -> M*pad4(ke); B block (ke x N) -> N*pad4(ke).
+__global__ void k_plane_sizes(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                              const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs, int a_side,
+                              int64_t* __restrict__ sz) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      const int rb = row_bs[r], cb = col_bs[col[b]];
+      sz[b] = a_side ? (int64_t)rb * pad4(cb) : (int64_t)cb * pad4(rb);
+    }
+}
+
+// Digits of one block into every plane.  a_side: x(p, kc) = A(p,kc) 2^-ea_p,
+// stored at [p][kc]; else x(c, kc) = B(kc,c) 2^-eb_c, stored at [c][kc].
+__global__ void k_digits(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                         const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                         const int8_t* __restrict__ col_bs, const double* __restrict__ d,
+                         const int64_t* __restrict__ rbase, const int64_t* __restrict__ cbase,
+                         const int* __restrict__ e_row, const int* __restrict__ e_col, int a_side,
+                         const int64_t* __restrict__ soff, int64_t plane_bytes, int s, int8_t* __restrict__ planes) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
+    const int rb = row_bs[r];
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      const int j = col[b], cb = col_bs[j];
+      const double* x = d + off[b];
+      const int lines = a_side ? rb : cb;  // stored rows
+      const int ke = a_side ? cb : rb;     // inner size
+      const int kp = pad4(ke);
+      for (int e = lane; e < lines * kp; e += 32) {
+        const int ln = e / kp, kc = e % kp;
+        double v = 0.0;
+        if (kc < ke) {
+          v = a_side ? x[(int64_t)kc * rb + ln] : x[(int64_t)ln * rb + kc];
+          v = ldexp(v, -(a_side ? e_row[rbase[r] + ln] : e_col[cbase[j] + ln]));
+        }
+        // digits: 2^6 v, then 7 bits per step; every step is exact in FP64
+        double t = ldexp(v, 6);
+        for (int p = 0; p < s; ++p) {
+          const double dg = rint(t);
+          planes[(int64_t)p * plane_bytes + soff[b] + e] = (int8_t)dg;
+          t = ldexp(t - dg, 7);
+        }
+      }
+    }
+  }
+}
+
+// ---- numeric kernel ---------------------------------------------------------------------
+struct WordRef {
+  const int* pa;            // A plane 0 word (row 0, this word)
+  unsigned long long pbk;   // B plane 0 word (col 0, this word) | row stride in words << 56
+};
+
+__device__ __forceinline__ void imma16832(int (&c)[4], const int (&a)[4], const int (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Word table of one chunk: words of every entry's plane-0 blocks, concatenated.
+__device__ __forceinline__ int build_words(const int* __restrict__ pa0, const int* __restrict__ pb0,
+                                           const Ent* __restrict__ ent, int64_t first, int m,
+                                           WordRef* __restrict__ tbl, int lane) {
+  Ent x{0, 0};
+  if (lane < m) x = ent[first + lane];
+  const int ke = lane < m ? (int)((unsigned long long)x.a >> 56) : 0;
+  const int nw = (ke + 3) >> 2;
+  const int incl = warp_incl_scan(nw, lane);
+  const int W = __shfl_sync(0xffffffffu, incl, 31);
+  const int* pa = pa0 + ((x.a & kOffMask) >> 2);
+  const int* pb = pb0 + (x.b >> 2);
+  const unsigned long long sb = (unsigned long long)nw << 56;
+  for (int w = 0, k = incl - nw; w < nw; ++w, ++k) tbl[k] = WordRef{pa + w, (unsigned long long)(pb + w) | sb};
+  __syncwarp();
+  return W;
+}
+
+// 16 tile rows (r0..) x 8 tile columns (c0..) of one C block.  SWAP: tile rows
+// are the block's columns (B side), tile columns the block's rows (A side).
+template <bool SWAP>
+__device__ __forceinline__ void mixed_tile(const int* __restrict__ pa0, const int* __restrict__ pb0,
+                                           int64_t a_plane_w, int64_t b_plane_w, int s,
+                                           const Ent* __restrict__ ent, int64_t s0, int n, int cap,
+                                           WordRef* __restrict__ tbl, int TM, int TN, int r0, int c0,
+                                           double (&out)[4]) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int ra = r0 + g, rb = r0 + g + 8, cc = c0 + g;
+  const bool ok_a = ra < TM, ok_b = rb < TM, ok_c = cc < TN;
+#pragma unroll
+  for (int h = 0; h < 4; ++h) out[h] = 0.0;
+  for (int p = 0; p < s; ++p) {
+    const int nq = s - p;  // q = 0 .. s-1-p  (p + q <= s - 1 in 0-based digits)
+    int acc[kMaxSlices][4];
+#pragma unroll
+    for (int q = 0; q < kMaxSlices; ++q)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) acc[q][h] = 0;
+    for (int base = 0; base < n; base += cap) {
+      const int m = min(cap, n - base);
+      const int W = build_words(pa0, pb0, ent, s0 + base, m, tbl, lane);
+      for (int w0 = 0; w0 < W; w0 += 8) {
+        int a[4];
+        int bq[2];
+        const int wa = w0 + t, wb = w0 + 4 + t;
+        const bool va = wa < W, vb = wb < W;
+        const WordRef ta = tbl[va ? wa : 0], tb = tbl[vb ? wb : 0];
+        const int sa = (int)(ta.pbk >> 56), sbw = (int)(tb.pbk >> 56);
+        const int* pba = reinterpret_cast<const int*>(ta.pbk & kOffMask);
+        const int* pbb = reinterpret_cast<const int*>(tb.pbk & kOffMask);
+        // tile op1 = A rows (or B columns when SWAP), plane p
+        const int* o1a = SWAP ? pba + (int64_t)p * b_plane_w : ta.pa + (int64_t)p * a_plane_w;
+        const int* o1b = SWAP ? pbb + (int64_t)p * b_plane_w : tb.pa + (int64_t)p * a_plane_w;
+        a[0] = (va && ok_a) ? __ldg(o1a + (int64_t)ra * sa) : 0;
+        a[1] = (va && ok_b) ? __ldg(o1a + (int64_t)rb * sa) : 0;
+        a[2] = (vb && ok_a) ? __ldg(o1b + (int64_t)ra * sbw) : 0;
+        a[3] = (vb && ok_b) ? __ldg(o1b + (int64_t)rb * sbw) : 0;
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q) {
+          if (q < nq) {
+            const int* o2a = SWAP ? ta.pa + (int64_t)q * a_plane_w : pba + (int64_t)q * b_plane_w;
+            const int* o2b = SWAP ? tb.pa + (int64_t)q * a_plane_w : pbb + (int64_t)q * b_plane_w;
+            bq[0] = (va && ok_c) ? __ldg(o2a + (int64_t)cc * sa) : 0;
+            bq[1] = (vb && ok_c) ? __ldg(o2b + (int64_t)cc * sbw) : 0;
+            imma16832(acc[q], a, bq);
+          }
+        }
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int q = 0; q < kMaxSlices; ++q)
+      if (q < nq) {
+        const int sh = -12 - 7 * (p + q);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) out[h] += ldexp((double)acc[q][h], sh);
+      }
+  }
+}
+
+__global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
+    int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
+    const int32_t* __restrict__ c_row, const int32_t* __restrict__ c_col, const Ent* __restrict__ ent,
+    const int* __restrict__ pa0, const int* __restrict__ pb0, int64_t a_plane_w, int64_t b_plane_w, int s,
+    const int64_t* __restrict__ rbase, const int64_t* __restrict__ cbase, const int* __restrict__ ea,
+    const int* __restrict__ eb, double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_words) {
+  extern __shared__ WordRef wtbl[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  WordRef* tbl = wtbl + (size_t)w * tbl_words;
+  const int64_t nwarps = (int64_t)gridDim.x * kMixWarps;
+  for (int64_t v = (int64_t)blockIdx.x * kMixWarps + w; v < n_work; v += nwarps) {
+    const Work it = work[v];
+    const int64_t c = work_c[v];
+    const int64_t o_off = it.lo & kMask40;
+    const int M = (int)((it.lo >> 40) & 0xff), N = (int)((it.lo >> 48) & 0xff);
+    const int64_t s0 = it.hi & kMask40;
+    const int n = (int)((unsigned long long)it.hi >> 40);
+    const int64_t rb0 = rbase[c_row[c]], cb0 = cbase[c_col[c]];
+    const bool swap = M <= 8 && N > 8;
+    const int TM = swap ? N : M, TN = swap ? M : N;
+    double sq = 0.0;
+    for (int r0 = 0; r0 < TM; r0 += 16)
+      for (int c0 = 0; c0 < TN; c0 += 8) {
+        double o[4];
+        if (swap)
+          mixed_tile<true>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+        else
+          mixed_tile<false>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const int tr = r0 + g + 8 * (h >> 1), tc = c0 + 2 * t + (h & 1);
+          if (tr < TM && tc < TN) {
+            const int r = swap ? tc : tr, cl = swap ? tr : tc;
+            const double val = ldexp(o[h], ea[rb0 + r] + eb[cb0 + cl]);
+            out[o_off + (int64_t)cl * M + r] = val;
+            sq = __fma_rn(val, val, sq);
+          }
+        }
+      }
+    sq = warp_sum(sq);
+    if (lane == 0 && out_nrm) out_nrm[c] = __dsqrt_rn(sq);
+  }
+}
+
+// ---- host side ----------------------------------------------------------------------------
+int mixed_slices_from_env() {
+  const char* v = getenv("LAMB_GPU_MIXED_SLICES");
+  int s = v ? atoi(v) : 7;
+  return std::max(2, std::min(s, kMaxSlices));
+}
+
+static std::vector<int64_t> elem_base(const std::vector<int8_t>& bs) {
+  std::vector<int64_t> b(bs.size() + 1, 0);
+  for (size_t i = 0; i < bs.size(); ++i) b[i + 1] = b[i] + bs[i];
+  return b;
+}
+
+int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp) {
+  if (max_block(A->h_row_bs) > 127 || max_block(B->h_col_bs) > 127)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "mixed: block too large");
+  mp->s = s;
+  const auto ra = elem_base(A->h_row_bs), cbv = elem_base(B->h_col_bs);
+  LAMB_TRY(dalloc(ctx, &mp->rbase, (int64_t)ra.size()));
+  LAMB_TRY(dalloc(ctx, &mp->cbase, (int64_t)cbv.size()));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(mp->rbase, ra.data(), sizeof(int64_t) * ra.size(), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(mp->cbase, cbv.data(), sizeof(int64_t) * cbv.size(), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_TRY(dalloc(ctx, &mp->ea, std::max<int64_t>(ra.back(), 1)));
+  LAMB_TRY(dalloc(ctx, &mp->eb, std::max<int64_t>(cbv.back(), 1)));
+  // eb starts at 0x80808080 (byte fill), below any frexp exponent, for the atomic max
+  LAMB_CUDA(ctx, cudaMemsetAsync(mp->eb, 0x80, sizeof(int) * std::max<int64_t>(cbv.back(), 1), ctx->stream));
+  if (A->nnz) {
+    k_row_exp<<<grid_for((int64_t)A->n_rows * 32), kThreads, 0, ctx->stream>>>(
+        A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, mp->rbase, mp->ea);
+    LAMB_LAUNCHED(ctx);
+  }
+  if (B->nnz) {
+    k_col_exp<<<grid_for(B->n_rows, 128), 128, 0, ctx->stream>>>(B->n_rows, B->row_p, B->col, B->off, B->row_bs,
+                                                                   B->col_bs, B->data, mp->cbase, mp->eb);
+    LAMB_LAUNCHED(ctx);
+  }
+  // plane offsets
+  int64_t* sz = nullptr;
+  LAMB_TRY(dalloc(ctx, &mp->a_soff, std::max<int64_t>(A->nnz, 1) + 1));
+  LAMB_TRY(dalloc(ctx, &mp->b_soff, std::max<int64_t>(B->nnz, 1) + 1));
+  LAMB_TRY(dalloc(ctx, &sz, std::max(A->nnz, B->nnz) + 1));
+  auto plane = [&](const DevMatrix* m, int a_side, int64_t* soff, int64_t* bytes) -> int32_t {
+    LAMB_CUDA(ctx, cudaMemsetAsync(sz + m->nnz, 0, sizeof(int64_t), ctx->stream));
+    if (m->nnz) {
+      k_plane_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->row_bs,
+                                                                         m->col_bs, a_side, sz);
+      LAMB_LAUNCHED(ctx);
+    }
+    LAMB_TRY(exclusive_scan_i64(ctx, sz, soff, m->nnz + 1));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(bytes, soff + m->nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *bytes = std::max<int64_t>((*bytes + 15) & ~15ll, 16);
+    return LAMB_GPU_OK;
+  };
+  LAMB_TRY(plane(A, 1, mp->a_soff, &mp->a_plane));
+  LAMB_TRY(plane(B, 0, mp->b_soff, &mp->b_plane));
+  dfree(ctx, sz);
+  LAMB_TRY(dalloc(ctx, &mp->a_planes, mp->a_plane * s));
+  LAMB_TRY(dalloc(ctx, &mp->b_planes, mp->b_plane * s));
+  if (A->nnz) {
+    k_digits<<<grid_for((int64_t)A->n_rows * 32), kThreads, 0, ctx->stream>>>(
+        A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, mp->rbase, nullptr, mp->ea, nullptr, 1,
+        mp->a_soff, mp->a_plane, s, mp->a_planes);
+    LAMB_LAUNCHED(ctx);
+  }
+  if (B->nnz) {
+    k_digits<<<grid_for((int64_t)B->n_rows * 32), kThreads, 0, ctx->stream>>>(
+        B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, nullptr, mp->cbase, nullptr, mp->eb, 0,
+        mp->b_soff, mp->b_plane, s, mp->b_planes);
+    LAMB_LAUNCHED(ctx);
+  }
+  return LAMB_GPU_OK;
+}
+
+void free_slices(Ctx* ctx, MixedPlanes* mp) {
+  dfree(ctx, mp->rbase); dfree(ctx, mp->cbase); dfree(ctx, mp->ea); dfree(ctx, mp->eb);
+  dfree(ctx, mp->a_soff); dfree(ctx, mp->b_soff); dfree(ctx, mp->a_planes); dfree(ctx, mp->b_planes);
+}
+
+// (plane offset | inner size << 56) for every A block; plane offsets of B.
+__global__ void k_pack_plane_meta(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                                  const int8_t* __restrict__ col_bs, const int64_t* __restrict__ soff,
+                                  int64_t* __restrict__ out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) out[b] = soff[b] | ((int64_t)col_bs[col[b]] << 56);
+}
+
+int32_t pack_plane_meta(Ctx* ctx, const DevMatrix* A, const MixedPlanes& mp, int64_t** a_meta) {
+  LAMB_TRY(dalloc(ctx, a_meta, std::max<int64_t>(A->nnz, 1)));
+  if (A->nnz) {
+    k_pack_plane_meta<<<grid_for(A->n_rows, 128), 128, 0, ctx->stream>>>(A->n_rows, A->row_p, A->col, A->col_bs,
+                                                                           mp.a_soff, *a_meta);
+    LAMB_LAUNCHED(ctx);
+  }
+  return LAMB_GPU_OK;
+}
+
+int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,
+                      const int32_t* work_c, double* c_nrm, const MixedPlanes& mp) {
+  if (sym.c_nnz == 0) return LAMB_GPU_OK;
+  const int mi = std::max(1, std::min(max_block(A->h_col_bs), 127));
+  const int wpe = (mi + 3) / 4;  // words per entry at most
+  const int cap = std::max(1, std::min(32, 4096 / wpe));
+  const int tbl_words = cap * wpe;
+  const size_t smem = sizeof(WordRef) * (size_t)tbl_words * kMixWarps;
+  if (smem > 48 * 1024)
+    LAMB_CUDA(ctx, cudaFuncSetAttribute(k_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mixed, kMixWarps * 32, smem));
+  const int64_t need = (sym.c_nnz + kMixWarps - 1) / kMixWarps;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * std::max(per_sm, 1)));
+  k_mixed<<<grid, kMixWarps * 32, smem, ctx->stream>>>(
+      sym.c_nnz, work, work_c, sym.c_row, C->col, sym.ent, reinterpret_cast<const int*>(mp.a_planes),
+      reinterpret_cast<const int*>(mp.b_planes), mp.a_plane / 4, mp.b_plane / 4, mp.s, mp.rbase, mp.cbase, mp.ea,
+      mp.eb, C->data, c_nrm, cap, tbl_words);
+  LAMB_LAUNCHED(ctx);
+  return LAMB_GPU_OK;
 }
 
 }  // namespace lamb

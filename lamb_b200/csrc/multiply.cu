@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
 }
 
 int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, bool want_ids,
-                       const int64_t* a_offk, Symbolic* out) {
+                       const int64_t* a_offk, Symbolic* out, const int64_t* b_meta) {
   out->c_nnz = out->n_ent = out->n_pairs = 0;
   out->flops = 0;
   LAMB_TRY(check_compatible(ctx, A, B));
@@ -277,7 +277,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
       LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
     kern<<<grid, kSymThreads, smem_fill, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms,
                                                         eps, fl, n_words, C->row_p, s_row_base, C->col, out->stack_p,
-                                                        a_offk, B->off, out->ent, out->ids);
+                                                        a_offk, b_meta ? b_meta : B->off, out->ent, out->ids);
     LAMB_LAUNCHED(ctx);
   }
   LAMB_TRY(dalloc(ctx, &out->c_row, std::max<int64_t>(C->nnz, 1)));
@@ -444,16 +444,25 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   int32_t* work_c = nullptr;
   int slices = 0;
   int64_t dropped = 0;
+  MixedPlanes mp;
+  const bool mixed = (flags & LAMB_GPU_MIXED) != 0;
   auto body = [&]() -> int32_t {
     LAMB_TRY(check_compatible(ctx, A, B));
     LAMB_TRY(ensure_row_order(ctx, A));
-    LAMB_TRY(pack_offk(ctx, A, true, &a_offk));
-    LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
+    if (mixed) {
+      slices = mixed_slices_from_env();
+      LAMB_TRY(build_slices(ctx, A, B, slices, &mp));
+      LAMB_TRY(pack_plane_meta(ctx, A, mp, &a_offk));
+      LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym, mp.b_soff));
+    } else {
+      LAMB_TRY(pack_offk(ctx, A, true, &a_offk));
+      LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
+    }
     LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c));
     LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
-    if (flags & LAMB_GPU_MIXED)
-      LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, &slices));
+    if (mixed)
+      LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, mp));
     else
       LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false,
                               max_block(A->h_col_bs)));
@@ -463,6 +472,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
     return LAMB_GPU_OK;
   };
   int32_t rc = body();
+  free_slices(ctx, &mp);
   dfree(ctx, a_offk);
   dfree(ctx, c_nrm);
   dfree(ctx, work);

@@ -46,8 +46,9 @@ int32_t check_compatible(Ctx* ctx, const DevMatrix* A, const DevMatrix* B);
 int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk);
 // Builds C's pattern (row_p, col, sector-major off, data buffer) and the
 // stacks; a_offk is required unless want_ids.
+// b_meta: operand-2 offsets written into the entries (null: B's data offsets).
 int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, bool want_ids,
-                       const int64_t* a_offk, Symbolic* out);
+                       const int64_t* a_offk, Symbolic* out, const int64_t* b_meta = nullptr);
 // Work list of C blocks in the row processing order of `order_src` (its h_order).
 int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
                    int32_t** work_c);
@@ -62,8 +63,21 @@ inline int max_block(const std::vector<int8_t>& v) {
   for (int8_t x : v) m = x > m ? x : m;
   return m;
 }
+// int8 digit planes of A (rows scaled by 2^ea) and B (columns scaled by 2^eb).
+struct MixedPlanes {
+  int s = 0;
+  int64_t *rbase = nullptr, *cbase = nullptr;  // element row / column bases
+  int *ea = nullptr, *eb = nullptr;            // row / column exponents
+  int64_t *a_soff = nullptr, *b_soff = nullptr;  // byte offset of every block in a plane
+  int64_t a_plane = 0, b_plane = 0;              // bytes per plane
+  int8_t *a_planes = nullptr, *b_planes = nullptr;
+};
+int mixed_slices_from_env();
+int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp);
+void free_slices(Ctx* ctx, MixedPlanes* mp);
+int32_t pack_plane_meta(Ctx* ctx, const DevMatrix* A, const MixedPlanes& mp, int64_t** a_meta);
 int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,
-                      const int32_t* work_c, double* c_nrm, int* slices_used);
+                      const int32_t* work_c, double* c_nrm, const MixedPlanes& mp);
 // Drops C blocks with c_nrm < eps from the index (data stay in place).
 int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps, int64_t* dropped);
 // Full multiply on device handles (used by the C ABI, purification and batches).

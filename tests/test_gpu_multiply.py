@@ -209,3 +209,28 @@ def test_block_size_classes(gpu_ctx, blk_o, blk_h):
     c, _ = _gpu_mult(gpu_ctx, a, b, 0.0)
     assert_same_pattern(c, c_ref)
     assert rel_frobenius_error(c, c_ref) <= TOL_FP64
+
+
+@pytest.mark.parametrize("slices,tol", [(7, 1e-11), (6, 1e-9)])
+def test_mixed_precision_error(gpu_ctx, monkeypatch, slices, tol):
+    """int8 split-slice products: same pattern as FP64, error against the
+    long-double oracle within the stated bound."""
+    monkeypatch.setenv("LAMB_GPU_MIXED_SLICES", str(slices))
+    g = WaterGeometry(96, None, 7.0, seed=21)
+    a, b = g.matrix(1), g.matrix(2)
+    c_ld, _ = oracle.multiply(a, b, 1e-10, oracle.LONG_DOUBLE)
+    c, st = _gpu_mult(gpu_ctx, a, b, 1e-10, gpu.MIXED)
+    assert st["mixed_slices"] == slices
+    assert_same_pattern(c, c_ld)
+    err = rel_frobenius_error(c, c_ld)
+    assert err <= tol, err
+
+
+def test_mixed_precision_random_fill(gpu_ctx, monkeypatch):
+    monkeypatch.setenv("LAMB_GPU_MIXED_SLICES", "7")
+    a = random_fill_matrix(5)
+    b = _with_values(a, 9)
+    c_ld, _ = oracle.multiply(a, b, 0.0, oracle.LONG_DOUBLE)
+    c, _ = _gpu_mult(gpu_ctx, a, b, 0.0, gpu.MIXED)
+    assert_same_pattern(c, c_ld)
+    assert rel_frobenius_error(c, c_ld) <= 1e-11
