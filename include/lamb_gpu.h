@@ -250,8 +250,15 @@ LAMB_API int32_t lamb_gpu_multiply_adjoint(lamb_gpu_ctx* ctx, lamb_gpu_matrix a,
 typedef struct lamb_gpu_batch lamb_gpu_batch;
 LAMB_API int32_t lamb_gpu_batch_create(lamb_gpu_ctx* ctx, const lamb_gpu_matrix* a, const lamb_gpu_matrix* b,
                               const lamb_gpu_matrix* c, int32_t n, double eps, lamb_gpu_batch** batch);
-/* Runs the batch once (first call captures the graph; later calls replay). */
+/* Runs the batch once (first call captures the graph; later calls replay).
+ * Product-filter decisions and C patterns are fixed at creation; executions
+ * recompute the block products from the current A/B values. */
 LAMB_API int32_t lamb_gpu_batch_execute(lamb_gpu_batch* batch, lamb_gpu_mult_stats* stats);
+/* Launch shape the autotuner picked at creation: warps per CTA, stack entries
+ * per column-table chunk, work items per queue fetch.  The choice is cached
+ * per problem signature in the process and, when LAMB_GPU_AUTOTUNE_CACHE
+ * names a file, across processes. */
+LAMB_API int32_t lamb_gpu_batch_config(const lamb_gpu_batch* batch, int32_t* warps, int32_t* cap, int32_t* grab);
 LAMB_API int32_t lamb_gpu_batch_destroy(lamb_gpu_batch* batch);
 
 /* ---- allocation-free entry point ------------------------------------------ */

@@ -58,6 +58,21 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
 int32_t run_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
                     const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2,
                     int max_inner);
+// Batched execution: operands of one instance, and a tunable launch shape.
+struct BatchInst {
+  const Ent* ent;
+  const double* a;
+  const double* b;
+  double* c;
+  double* nrm;
+};
+struct BatchConfig {
+  int warps = 8;  // warps per CTA (4 or 8)
+  int cap = 32;   // stack entries per column-table chunk
+  int grab = 4;   // work items per queue fetch
+};
+int32_t launch_batch(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const int32_t* work_i,
+                     const BatchInst* inst, unsigned long long* head, const BatchConfig& cfg, int max_inner);
 inline int max_block(const std::vector<int8_t>& v) {
   int m = 0;
   for (int8_t x : v) m = x > m ? x : m;

@@ -247,6 +247,40 @@ __device__ void block_generic(const double* __restrict__ d1, const double* __res
   if (lane == 0 && out_nrm) out_nrm[c] = __dsqrt_rn(sq);
 }
 
+// One work item: dispatch on the output block shape.
+template <bool TA, bool TB>
+__device__ __forceinline__ void process_item(const Work& it, int64_t c, const Ent* __restrict__ ent,
+                                             const double* __restrict__ d1, const double* __restrict__ d2,
+                                             double* __restrict__ out, double* __restrict__ out_nrm,
+                                             ColRef* __restrict__ tbl, int cap) {
+  const int64_t o_off = it.lo & kMask40;
+  const int M = (int)((it.lo >> 40) & 0xff), N = (int)((it.lo >> 48) & 0xff);
+  const int64_t s0 = it.hi & kMask40;
+  const int n = (int)((unsigned long long)it.hi >> 40);
+  if (M == 0 || N == 0) {
+    if ((threadIdx.x & 31) == 0 && out_nrm) out_nrm[c] = 0.0;
+    return;
+  }
+  if (M <= 8 && N <= 8) {
+    block_m8<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap);
+  } else if (M <= 8 && N <= 32) {
+    for (int r0 = 0; r0 < N; r0 += 16)
+      block_m16<1, TA, TB, true>(d1, d2, out, out_nrm, c, M, N, r0, 0, o_off, s0, n, ent, tbl, cap, r0 + 16 >= N);
+  } else if (M <= 32 && N <= 32) {
+    // 16-row x 16-column slabs (the last may be 8 columns wide)
+    for (int r0 = 0; r0 < M; r0 += 16)
+      for (int c0 = 0; c0 < N; c0 += 16) {
+        const bool last = r0 + 16 >= M && c0 + 16 >= N;
+        if (N - c0 > 8)
+          block_m16<2, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
+        else
+          block_m16<1, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
+      }
+  } else {
+    block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent);
+  }
+}
+
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(kNumWarps * 32, 3)
     k_stacked(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
@@ -256,37 +290,59 @@ __global__ void __launch_bounds__(kNumWarps * 32, 3)
   const int w = threadIdx.x >> 5;
   ColRef* tbl = tbl_all + (size_t)w * tbl_cols;
   const int64_t nwarps = (int64_t)gridDim.x * kNumWarps;
-  for (int64_t v = (int64_t)blockIdx.x * kNumWarps + w; v < n_work; v += nwarps) {
-    const Work it = work[v];
-    const int64_t c = work_c[v];
-    const int64_t o_off = it.lo & kMask40;
-    const int M = (int)((it.lo >> 40) & 0xff), N = (int)((it.lo >> 48) & 0xff);
-    const int64_t s0 = it.hi & kMask40;
-    const int n = (int)((unsigned long long)it.hi >> 40);
-    if (M == 0 || N == 0) {
-      if ((threadIdx.x & 31) == 0 && out_nrm) out_nrm[c] = 0.0;
-      continue;
-    }
-    const int nf = (N + 7) >> 3;
-    if (M <= 8 && N <= 8) {
-      block_m8<1, TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap);
-    } else if (M <= 8 && N <= 32) {
-      for (int r0 = 0; r0 < N; r0 += 16)
-        block_m16<1, TA, TB, true>(d1, d2, out, out_nrm, c, M, N, r0, 0, o_off, s0, n, ent, tbl, cap, r0 + 16 >= N);
-    } else if (M <= 32 && N <= 32) {
-      // 16-row x 16-column slabs (the last may be 8 columns wide)
-      for (int r0 = 0; r0 < M; r0 += 16)
-        for (int c0 = 0; c0 < N; c0 += 16) {
-          const bool last = r0 + 16 >= M && c0 + 16 >= N;
-          if (N - c0 > 8)
-            block_m16<2, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
-          else
-            block_m16<1, TA, TB, false>(d1, d2, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
-        }
-    } else {
-      block_generic<TA, TB>(d1, d2, out, out_nrm, c, M, N, o_off, s0, n, ent);
+  for (int64_t v = (int64_t)blockIdx.x * kNumWarps + w; v < n_work; v += nwarps)
+    process_item<TA, TB>(work[v], work_c[v], ent, d1, d2, out, out_nrm, tbl, cap);
+}
+
+// Persistent kernel over the global queue of a batch: warps take `grab`
+// consecutive items per atomic on `head` (reset before every launch); each
+// item names its instance, whose operands come from the instance table.
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, 24 / NW)
+    k_stacked_batch(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
+                    const int32_t* __restrict__ work_i, const BatchInst* __restrict__ inst,
+                    unsigned long long* __restrict__ head, int grab, int cap, int tbl_cols) {
+  extern __shared__ ColRef tbl_all[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  ColRef* tbl = tbl_all + (size_t)w * tbl_cols;
+  while (true) {
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(head, (unsigned long long)grab);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if (start >= (unsigned long long)n_work) break;
+    const int64_t end = min((int64_t)start + grab, n_work);
+    for (int64_t v = (int64_t)start; v < end; ++v) {
+      const BatchInst I = inst[work_i[v]];
+      process_item<false, false>(work[v], work_c[v], I.ent, I.a, I.b, I.c, I.nrm, tbl, cap);
     }
   }
+}
+
+template <int NW>
+static int32_t launch_batch_nw(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c,
+                               const int32_t* work_i, const BatchInst* inst, unsigned long long* head, int grab,
+                               int cap, int max_inner) {
+  const int mi = std::max(1, std::min(max_inner, 127));
+  cap = std::max(1, std::min(cap, 8192 / mi));
+  const int tbl_cols = cap * mi;
+  const size_t smem = sizeof(ColRef) * (size_t)tbl_cols * NW;
+  auto kern = k_stacked_batch<NW>;
+  if (smem > 48 * 1024)
+    LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem));
+  const int grid = sms * std::max(per_sm, 1);
+  kern<<<grid, NW * 32, smem, ctx->stream>>>(n_work, work, work_c, work_i, inst, head, grab, cap, tbl_cols);
+  LAMB_LAUNCHED(ctx);
+  return LAMB_GPU_OK;
+}
+
+int32_t launch_batch(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const int32_t* work_i,
+                     const BatchInst* inst, unsigned long long* head, const BatchConfig& cfg, int max_inner) {
+  if (n_work == 0) return LAMB_GPU_OK;
+  if (cfg.warps == 4) return launch_batch_nw<4>(ctx, n_work, work, work_c, work_i, inst, head, cfg.grab, cfg.cap, max_inner);
+  return launch_batch_nw<8>(ctx, n_work, work, work_c, work_i, inst, head, cfg.grab, cfg.cap, max_inner);
 }
 
 template <bool TA, bool TB>

@@ -79,6 +79,7 @@ def lib() -> C.CDLL:
             "lamb_gpu_batch_create": [vp, P(i64), P(i64), P(i64), i32, dbl, P(vp)],
             "lamb_gpu_batch_execute": [vp, P(MultStats)],
             "lamb_gpu_batch_destroy": [vp],
+            "lamb_gpu_batch_config": [vp, P(i32), P(i32), P(i32)],
         }
         for name, args in sig.items():
             f = getattr(L, name, None)
@@ -187,6 +188,15 @@ class Context:
         """da := (dc . b^T) on a's pattern, db := (a^T . dc) on b's pattern."""
         self.check(lib().lamb_gpu_multiply_adjoint(self._h, a.h, b.h, dc.h, da.h if da else 0, db.h if db else 0))
 
+    def batch(self, a: Sequence["DeviceMatrix"], b: Sequence["DeviceMatrix"], c: Sequence["DeviceMatrix"],
+              eps: float = 0.0) -> "Batch":
+        """Independent C_i = A_i . B_i in one persistent launch (graph-replayed)."""
+        n = len(a)
+        arr = lambda ms: (C.c_int64 * n)(*[m.h for m in ms])
+        h = C.c_void_p()
+        self.check(lib().lamb_gpu_batch_create(self._h, arr(a), arr(b), arr(c), n, eps, C.byref(h)))
+        return Batch(self, h)
+
     def stacks(self, a: "DeviceMatrix", b: "DeviceMatrix", c: "DeviceMatrix", eps: float = 0.0,
                flags: int = 0) -> np.ndarray:
         n = C.c_int64(0)
@@ -194,6 +204,28 @@ class Context:
         out = np.zeros((max(n.value, 1), 5), np.int64)
         self.check(lib().lamb_gpu_multiply_stacks(self._h, a.h, b.h, c.h, eps, flags, out.ctypes.data, C.byref(n)))
         return out[:n.value]
+
+
+class Batch:
+    """A created batch (lamb_gpu_batch)."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx, self.h = ctx, h
+
+    def execute(self) -> dict:
+        st = MultStats()
+        self.ctx.check(lib().lamb_gpu_batch_execute(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def config(self) -> dict:
+        w, c, g = C.c_int32(), C.c_int32(), C.c_int32()
+        self.ctx.check(lib().lamb_gpu_batch_config(self.h, C.byref(w), C.byref(c), C.byref(g)))
+        return {"warps": w.value, "cap": c.value, "grab": g.value}
+
+    def destroy(self) -> None:
+        if self.h:
+            lib().lamb_gpu_batch_destroy(self.h)
+            self.h = None
 
 
 class DeviceMatrix:
