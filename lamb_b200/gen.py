@@ -185,16 +185,20 @@ def random_fill_matrix(seed: int, n_atoms: Optional[int] = None, max_atoms: int 
 
 
 def gapped_hamiltonian(geom: "WaterGeometry", seed: int, gap: float = 0.2, occ_fraction: float = 0.3,
-                       decay: float = 1.5) -> LambMatrix:
+                       decay: float = 1.5, coupling: float = 1.0) -> LambMatrix:
     """Symmetric block-sparse H on the geometry's pattern with a spectral gap
     of at least `gap` around mu = 0.
 
-    H = V + D: V is the symmetric water matrix (entries u*exp(-r/decay),
-    diagonal blocks (X+X^T)/2 + I); D is diagonal with d_p = -(gap/2 + R_p)
-    for the first round(occ_fraction*b) functions of every atom (occupied)
-    and +(gap/2 + R_p) for the rest, R_p = sum_q |V_pq| (row p of V).  Every
-    Gershgorin disc of H then lies outside (-gap/2, gap/2)."""
+    H = s*V + D: V is the symmetric water matrix (entries u*exp(-r/decay),
+    diagonal blocks (X+X^T)/2 + I), s = `coupling`; D is diagonal with
+    d_p = -(gap/2 + R_p) for the first round(occ_fraction*b) functions of
+    every atom (occupied) and +(gap/2 + R_p) for the rest,
+    R_p = sum_q |s*V_pq| (row p of s*V).  Every Gershgorin disc of H then lies
+    outside (-gap/2, gap/2)."""
     v = geom.matrix(seed, decay, symmetric=True, name="H")
+    if coupling != 1.0:
+        for s_ in v.sectors:
+            s_.data *= coupling
     # row sums of |V| per element row, per subset
     sub_sizes = v.subset_blk_sizes(0)
     offs = [np.concatenate([[0], np.cumsum(b.astype(np.int64))]) for b in sub_sizes]

@@ -78,7 +78,7 @@ def _dense_purify_loss(hv, ra, ca, n, lam, K, mu=0.0):
 
 def test_purification_gradient_checkpointed(gpu_ctx):
     g = WaterGeometry(16, None, 4.5, seed=6)
-    h = gapped_hamiltonian(g, 3)
+    h = gapped_hamiltonian(g, 3, coupling=0.05)
     K, cp = 6, 2
     lam = AG.gershgorin_lambda(h)
     eng = AG.PurifyEngine(gpu_ctx, K, lam, checkpoint=cp)
