@@ -270,14 +270,14 @@ int32_t scale_shift_impl(Ctx* ctx, DevMatrix* X, double alpha, double shift) {
       k_scale<<<grid_for(X->data_len), kThreads, 0, ctx->stream>>>(X->data_len, X->data, alpha);
       LAMB_LAUNCHED(ctx);
     }
-    invalidate_values(ctx, X);
+    X->norms_valid = false;
     return LAMB_GPU_OK;
   }
   DevMatrix I;
   int32_t rc = identity_like(ctx, X, &I);
   if (rc == LAMB_GPU_OK) rc = axpby_impl(ctx, shift, &I, alpha, X);
   free_matrix_buffers(ctx, &I);
-  invalidate_values(ctx, X);
+  X->norms_valid = false;
   return rc;
 }
 

@@ -48,17 +48,7 @@ struct DevMatrix {
   float box[3] = {0, 0, 0};
   std::vector<int32_t> h_order;  // row processing order, empty until computed
   int32_t* order = nullptr;      // device copy of h_order
-  // Packed operand copies for the numeric kernel, valid until the values change:
-  // [0] every block row-major with its inner (column) size padded to 4;
-  // [1] every block column-major with its inner (row) size padded to 4.
-  // Block starts are 32-byte aligned; pk_off gives each block's start.
-  double* pk[2] = {nullptr, nullptr};
-  int64_t* pk_off[2] = {nullptr, nullptr};
-  bool pk_valid[2] = {false, false};
 };
-
-// Marks the values of m as changed: cached norms and packed copies are dropped.
-void invalidate_values(struct Ctx* ctx, DevMatrix* m);
 
 struct Ctx {
   int device = 0;

@@ -34,16 +34,7 @@ void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
   dfree(ctx, m->norms);
   dfree(ctx, m->order);
   m->h_order.clear();
-  invalidate_values(ctx, m);
-}
-
-void invalidate_values(Ctx* ctx, DevMatrix* m) {
   m->norms_valid = false;
-  for (int s = 0; s < 2; ++s) {
-    dfree(ctx, m->pk[s]);
-    dfree(ctx, m->pk_off[s]);
-    m->pk_valid[s] = false;
-  }
 }
 
 int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h) {

@@ -297,22 +297,6 @@ __global__ void k_pack_offk(int32_t n_rows, const int64_t* __restrict__ row_p, c
       out[b] = off[b] | ((int64_t)(k_is_col ? col_bs[col[b]] : row_bs[r]) << 56);
 }
 
-__global__ void k_pack_meta(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
-                            const int64_t* __restrict__ off, const int8_t* __restrict__ col_bs,
-                            int64_t* __restrict__ out) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) out[b] = off[b] | ((int64_t)col_bs[col[b]] << 56);
-}
-
-int32_t pack_meta(Ctx* ctx, const DevMatrix* m, const int64_t* off, int64_t** meta) {
-  LAMB_TRY(dalloc(ctx, meta, std::max<int64_t>(m->nnz, 1)));
-  if (m->nnz) {
-    k_pack_meta<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, off, m->col_bs, *meta);
-    LAMB_LAUNCHED(ctx);
-  }
-  return LAMB_GPU_OK;
-}
-
 int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk) {
   LAMB_TRY(dalloc(ctx, offk, std::max<int64_t>(m->nnz, 1)));
   if (m->data_len > kOffMask) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "operand data too large");
@@ -435,7 +419,7 @@ int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps, i
   C->row_p = d_nrp; C->col = ncol; C->off = noff;
   C->nnz = kept;
   C->sec_nblk = snb;
-  invalidate_values(ctx, C);
+  C->norms_valid = false;
   dfree(ctx, keep_rn); dfree(ctx, d_cb);
   return LAMB_GPU_OK;
 }
@@ -471,11 +455,8 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
       LAMB_TRY(pack_plane_meta(ctx, A, mp, &a_offk));
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym, mp.b_soff));
     } else {
-      // entries point into the packed copies: A row-major, B column-major
-      LAMB_TRY(ensure_packed(ctx, A, 0));
-      LAMB_TRY(ensure_packed(ctx, B, 1));
-      LAMB_TRY(pack_meta(ctx, A, A->pk_off[0], &a_offk));
-      LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym, B->pk_off[1]));
+      LAMB_TRY(pack_offk(ctx, A, true, &a_offk));
+      LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
     }
     LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c));
     LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
@@ -483,8 +464,8 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
     if (mixed)
       LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, mp));
     else
-      LAMB_TRY(run_stacked_packed(ctx, sym.c_nnz, work, work_c, sym.ent, A->pk[0], B->pk[1], C->data, c_nrm,
-                                  max_block(A->h_col_bs)));
+      LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false,
+                              max_block(A->h_col_bs)));
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps, &dropped));
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
@@ -498,7 +479,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   dfree(ctx, work_c);
   free_symbolic(ctx, sym);
   if (rc != LAMB_GPU_OK) return rc;
-  invalidate_values(ctx, C);
+  C->norms_valid = false;
   st.n_products = sym.n_ent;
   st.n_products_skipped = sym.n_pairs - sym.n_ent;
   st.n_c_blocks = C->nnz;

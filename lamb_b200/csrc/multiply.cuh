@@ -42,8 +42,6 @@ struct Symbolic {
 void free_symbolic(Ctx* ctx, Symbolic& s);
 
 int32_t check_compatible(Ctx* ctx, const DevMatrix* A, const DevMatrix* B);
-// (off[b] | column block size << 56) for every block of m.
-int32_t pack_meta(Ctx* ctx, const DevMatrix* m, const int64_t* off, int64_t** meta);
 // Packs (data offset | column block size << 56) for every block of m.
 int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk);
 // Builds C's pattern (row_p, col, sector-major off, data buffer) and the
@@ -60,10 +58,6 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
 int32_t run_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
                     const double* d1, const double* d2, double* out, double* out_nrm, bool t1, bool t2,
                     int max_inner);
-// Packed operand copies (DevMatrix::pk[side]) and the forward kernel on them.
-int32_t ensure_packed(Ctx* ctx, DevMatrix* m, int side);
-int32_t run_stacked_packed(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
-                           const double* apk, const double* bpk, double* out, double* out_nrm, int max_inner);
 // Batched execution: operands of one instance, and a tunable launch shape.
 struct BatchInst {
   const Ent* ent;

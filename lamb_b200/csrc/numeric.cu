@@ -345,288 +345,6 @@ int32_t launch_batch(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* 
   return launch_batch_nw<8>(ctx, n_work, work, work_c, work_i, inst, head, cfg.grab, cfg.cap, max_inner);
 }
 
-// ======================= packed-operand forward kernel ===========================
-// Operands come from the packed copies (DevMatrix::pk): A blocks row-major and
-// B blocks column-major, inner size padded to kp = pad4(ke), 32-byte aligned.
-// The inner dimension advances in quads (4 columns of one entry), so every
-// quad lies inside one block and a lane reads its 4 inner indices of one row
-// (A) or column (B) with two 16-byte loads.  The mma k-slots are permuted:
-// lane t's slots t, t+4, t+8, t+12 of a 16-wide window hold inner columns
-// 4t .. 4t+3 of the window's quad t, consistently for both operands.
-#ifndef PK_MIN_BLOCKS
-#define PK_MIN_BLOCKS 3
-#endif
-struct QuadRef {
-  const double* pa;        // A: row 0 of this quad
-  unsigned long long pbk;  // B: column 0 of this quad | kp << 56
-};
-
-__device__ __forceinline__ int build_quads(const double* __restrict__ apk, const double* __restrict__ bpk,
-                                           const Ent* __restrict__ ent, int64_t first, int m,
-                                           QuadRef* __restrict__ tbl, int lane) {
-  Ent x{0, 0};
-  if (lane < m) x = ent[first + lane];
-  const int ke = lane < m ? (int)((unsigned long long)x.a >> 56) : 0;
-  const int kp = (ke + 3) & ~3;
-  const int nq = kp >> 2;
-  const int incl = warp_incl_scan(nq, lane);
-  const int Q = __shfl_sync(0xffffffffu, incl, 31);
-  const double* pa = apk + (x.a & kOffMask);
-  const double* pb = bpk + x.b;
-  const unsigned long long kb = (unsigned long long)kp << 56;
-  for (int q = 0, w = incl - nq; q < nq; ++q, ++w) tbl[w] = QuadRef{pa + 4 * q, (unsigned long long)(pb + 4 * q) | kb};
-  __syncwarp();
-  return Q;
-}
-
-__device__ __forceinline__ double2 ld2(const double* p, bool ok) {
-  return ok ? __ldg(reinterpret_cast<const double2*>(p)) : make_double2(0.0, 0.0);
-}
-
-// 16 tile rows (r0..) x 8*NF tile columns (c0..); SWAP: tile rows are B columns.
-template <int NF, bool SWAP>
-__device__ __forceinline__ void pk_m16(const double* __restrict__ apk, const double* __restrict__ bpk,
-                                       double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M,
-                                       int N, int r0, int c0, int64_t o_off, int64_t s0, int n,
-                                       const Ent* __restrict__ ent, QuadRef* __restrict__ tbl, int cap,
-                                       bool last_slab) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const int TM = SWAP ? N : M, TN = SWAP ? M : N;
-  double acc[NF][4];
-#pragma unroll
-  for (int j = 0; j < NF; ++j)
-#pragma unroll
-    for (int h = 0; h < 4; ++h) acc[j][h] = 0.0;
-  const int ra = r0 + g, rb = r0 + g + 8;
-  const bool rok0 = ra < TM, rok1 = rb < TM;
-  bool cok[NF];
-#pragma unroll
-  for (int j = 0; j < NF; ++j) cok[j] = c0 + j * 8 + g < TN;
-  for (int base = 0; base < n; base += cap) {
-    const int m = min(cap, n - base);
-    const int Q = build_quads(apk, bpk, ent, s0 + base, m, tbl, lane);
-    for (int w0 = 0; w0 < Q; w0 += 4) {
-      const int w = w0 + t;
-      const bool qv = w < Q;
-      const QuadRef cr = tbl[qv ? w : 0];
-      const int kp = (int)(cr.pbk >> 56);
-      const double* pa = cr.pa;
-      const double* pb = reinterpret_cast<const double*>(cr.pbk & kOffMask);
-      const double* p1 = SWAP ? pb : pa;  // tile op1 rows
-      const double* p2 = SWAP ? pa : pb;  // tile op2 columns
-      const double2 a0 = ld2(p1 + (int64_t)ra * kp, qv && rok0), a1 = ld2(p1 + (int64_t)ra * kp + 2, qv && rok0);
-      const double2 b0 = ld2(p1 + (int64_t)rb * kp, qv && rok1), b1 = ld2(p1 + (int64_t)rb * kp + 2, qv && rok1);
-      const double a[8] = {a0.x, b0.x, a0.y, b0.y, a1.x, b1.x, a1.y, b1.y};
-#pragma unroll
-      for (int j = 0; j < NF; ++j) {
-        const int cc = c0 + j * 8 + g;
-        const double2 x0 = ld2(p2 + (int64_t)cc * kp, qv && cok[j]);
-        const double2 x1 = ld2(p2 + (int64_t)cc * kp + 2, qv && cok[j]);
-        const double bv[4] = {x0.x, x0.y, x1.x, x1.y};
-        dmma16816(acc[j], a, bv);
-      }
-    }
-    __syncwarp();
-  }
-  double sq = 0.0;
-#pragma unroll
-  for (int j = 0; j < NF; ++j)
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int r = r0 + g + 8 * (h >> 1), cc = c0 + j * 8 + 2 * t + (h & 1);
-      if (r < TM && cc < TN) {
-        const double v = acc[j][h];
-        if (SWAP)
-          out[o_off + (int64_t)r * M + cc] = v;
-        else
-          out[o_off + (int64_t)cc * M + r] = v;
-        sq = __fma_rn(v, v, sq);
-      }
-    }
-  sq = warp_sum(sq);
-  if (out_nrm) {
-    const double prev = (r0 == 0 && c0 == 0) ? 0.0 : out_nrm[c];
-    __syncwarp();
-    if (lane == 0) out_nrm[c] = last_slab ? __dsqrt_rn(prev + sq) : prev + sq;
-    __syncwarp();
-  }
-}
-
-// Blocks of at most 8 x 8: m8n8k4, one quad per mma, two quads per step.
-__device__ __forceinline__ void pk_m8(const double* __restrict__ apk, const double* __restrict__ bpk,
-                                      double* __restrict__ out, double* __restrict__ out_nrm, int64_t c, int M, int N,
-                                      int64_t o_off, int64_t s0, int n, const Ent* __restrict__ ent,
-                                      QuadRef* __restrict__ tbl, int cap) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  double c0 = 0.0, c1 = 0.0;
-  const bool rok = g < M, cok = g < N;
-  for (int base = 0; base < n; base += cap) {
-    const int m = min(cap, n - base);
-    const int Q = build_quads(apk, bpk, ent, s0 + base, m, tbl, lane);
-    for (int w = 0; w < Q; w += 2) {
-      double a[2], b[2];
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const bool qv = w + u < Q;
-        const QuadRef cr = tbl[qv ? w + u : 0];
-        const int kp = (int)(cr.pbk >> 56);
-        const double* pb = reinterpret_cast<const double*>(cr.pbk & kOffMask);
-        a[u] = (qv && rok) ? __ldg(cr.pa + (int64_t)g * kp + t) : 0.0;
-        b[u] = (qv && cok) ? __ldg(pb + (int64_t)g * kp + t) : 0.0;
-      }
-      dmma884(c0, c1, a[0], b[0]);
-      dmma884(c0, c1, a[1], b[1]);
-    }
-    __syncwarp();
-  }
-  double sq = 0.0;
-  const double v2[2] = {c0, c1};
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int cc = 2 * t + h;
-    if (g < M && cc < N) {
-      out[o_off + (int64_t)cc * M + g] = v2[h];
-      sq = __fma_rn(v2[h], v2[h], sq);
-    }
-  }
-  sq = warp_sum(sq);
-  if (lane == 0 && out_nrm) out_nrm[c] = __dsqrt_rn(sq);
-}
-
-__device__ __forceinline__ void process_item_pk(const Work& it, int64_t c, const Ent* __restrict__ ent,
-                                                const double* __restrict__ apk, const double* __restrict__ bpk,
-                                                double* __restrict__ out, double* __restrict__ out_nrm,
-                                                QuadRef* __restrict__ tbl, int cap) {
-  const int64_t o_off = it.lo & kMask40;
-  const int M = (int)((it.lo >> 40) & 0xff), N = (int)((it.lo >> 48) & 0xff);
-  const int64_t s0 = it.hi & kMask40;
-  const int n = (int)((unsigned long long)it.hi >> 40);
-  if (M == 0 || N == 0) {
-    if ((threadIdx.x & 31) == 0 && out_nrm) out_nrm[c] = 0.0;
-    return;
-  }
-  if (M <= 8 && N <= 8) {
-    pk_m8(apk, bpk, out, out_nrm, c, M, N, o_off, s0, n, ent, tbl, cap);
-  } else if (M <= 8) {
-    for (int r0 = 0; r0 < N; r0 += 16)
-      pk_m16<1, true>(apk, bpk, out, out_nrm, c, M, N, r0, 0, o_off, s0, n, ent, tbl, cap, r0 + 16 >= N);
-  } else {
-    for (int r0 = 0; r0 < M; r0 += 16)
-      for (int c0 = 0; c0 < N; c0 += 16) {
-        const bool last = r0 + 16 >= M && c0 + 16 >= N;
-        if (N - c0 > 8)
-          pk_m16<2, false>(apk, bpk, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
-        else
-          pk_m16<1, false>(apk, bpk, out, out_nrm, c, M, N, r0, c0, o_off, s0, n, ent, tbl, cap, last);
-      }
-  }
-}
-
-__global__ void __launch_bounds__(kNumWarps * 32, PK_MIN_BLOCKS)
-    k_stacked_pk(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
-                 const Ent* __restrict__ ent, const double* __restrict__ apk, const double* __restrict__ bpk,
-                 double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_quads) {
-  extern __shared__ QuadRef qtbl[];
-  const int w = threadIdx.x >> 5;
-  QuadRef* tbl = qtbl + (size_t)w * tbl_quads;
-  const int64_t nwarps = (int64_t)gridDim.x * kNumWarps;
-  for (int64_t v = (int64_t)blockIdx.x * kNumWarps + w; v < n_work; v += nwarps)
-    process_item_pk(work[v], work_c[v], ent, apk, bpk, out, out_nrm, tbl, cap);
-}
-
-int32_t run_stacked_packed(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
-                           const double* apk, const double* bpk, double* out, double* out_nrm, int max_inner) {
-  if (n_work == 0) return LAMB_GPU_OK;
-  const int mq = std::max(1, (std::min(max_inner, 127) + 3) / 4);
-  const int cap = std::max(1, std::min(kMaxChunk, 2048 / mq));
-  const int tbl_quads = cap * mq;
-  const size_t smem = sizeof(QuadRef) * (size_t)tbl_quads * kNumWarps;
-  if (smem > 48 * 1024)
-    LAMB_CUDA(ctx, cudaFuncSetAttribute(k_stacked_pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int sms = 148, per_sm = 1;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stacked_pk, kNumWarps * 32, smem));
-  const int64_t need = (n_work + kNumWarps - 1) / kNumWarps;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * std::max(per_sm, 1)));
-  k_stacked_pk<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, apk, bpk, out, out_nrm, cap,
-                                                           tbl_quads);
-  LAMB_LAUNCHED(ctx);
-  return LAMB_GPU_OK;
-}
-
-// ---- packing --------------------------------------------------------------------------
-// side 0: block (M x ke, column-major) -> M rows of kp; side 1: block (ke x N,
-// column-major) -> N columns of kp.  Padding is zero.
-__global__ void k_pack_sizes(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
-                             const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs, int side,
-                             int64_t* __restrict__ sz) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      const int rb = row_bs[r], cb = col_bs[col[b]];
-      sz[b] = side == 0 ? (int64_t)rb * ((cb + 3) & ~3) : (int64_t)cb * ((rb + 3) & ~3);
-    }
-}
-
-__global__ void k_pack(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
-                       const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
-                       const int8_t* __restrict__ col_bs, const double* __restrict__ d, int side,
-                       const int64_t* __restrict__ poff, double* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
-    const int rb = row_bs[r];
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      const int cb = col_bs[col[b]];
-      const double* x = d + off[b];
-      double* o = out + poff[b];
-      if (side == 0) {
-        const int kp = (cb + 3) & ~3;
-        for (int e = lane; e < rb * kp; e += 32) {
-          const int row = e / kp, kk = e % kp;
-          o[e] = kk < cb ? x[(int64_t)kk * rb + row] : 0.0;
-        }
-      } else {
-        const int kp = (rb + 3) & ~3;
-        for (int e = lane; e < cb * kp; e += 32) {
-          const int cl = e / kp, kk = e % kp;
-          o[e] = kk < rb ? x[(int64_t)cl * rb + kk] : 0.0;
-        }
-      }
-    }
-  }
-}
-
-int32_t ensure_packed(Ctx* ctx, DevMatrix* m, int side) {
-  if (m->pk_valid[side]) return LAMB_GPU_OK;
-  dfree(ctx, m->pk[side]);
-  dfree(ctx, m->pk_off[side]);
-  int64_t* sz = nullptr;
-  LAMB_TRY(dalloc(ctx, &sz, m->nnz + 1));
-  LAMB_TRY(dalloc(ctx, &m->pk_off[side], m->nnz + 1));
-  LAMB_CUDA(ctx, cudaMemsetAsync(sz + m->nnz, 0, sizeof(int64_t), ctx->stream));
-  if (m->nnz) {
-    k_pack_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->row_bs,
-                                                                      m->col_bs, side, sz);
-    LAMB_LAUNCHED(ctx);
-  }
-  LAMB_TRY(exclusive_scan_i64(ctx, sz, m->pk_off[side], m->nnz + 1));
-  int64_t total = 0;
-  LAMB_CUDA(ctx, cudaMemcpyAsync(&total, m->pk_off[side] + m->nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (total > kOffMask) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "packed operand too large");
-  LAMB_TRY(dalloc(ctx, &m->pk[side], std::max<int64_t>(total, 4)));
-  if (m->nnz) {
-    k_pack<<<grid_for((int64_t)m->n_rows * 32), kThreads, 0, ctx->stream>>>(
-        m->n_rows, m->row_p, m->col, m->off, m->row_bs, m->col_bs, m->data, side, m->pk_off[side], m->pk[side]);
-    LAMB_LAUNCHED(ctx);
-  }
-  dfree(ctx, sz);
-  m->pk_valid[side] = true;
-  return LAMB_GPU_OK;
-}
-
 template <bool TA, bool TB>
 static int32_t launch_stacked(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c, const Ent* ent,
                               const double* d1, const double* d2, double* out, double* out_nrm, int max_inner) {
