@@ -285,13 +285,18 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(kNumWarps * 32, 3)
     k_stacked(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
               const Ent* __restrict__ ent, const double* __restrict__ d1, const double* __restrict__ d2,
-              double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_cols) {
+              double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_cols,
+              unsigned long long* __restrict__ head) {
   extern __shared__ ColRef tbl_all[];
-  const int w = threadIdx.x >> 5;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ColRef* tbl = tbl_all + (size_t)w * tbl_cols;
-  const int64_t nwarps = (int64_t)gridDim.x * kNumWarps;
-  for (int64_t v = (int64_t)blockIdx.x * kNumWarps + w; v < n_work; v += nwarps)
+  while (true) {
+    unsigned long long v = 0;
+    if (lane == 0) v = atomicAdd(head, 1ull);
+    v = __shfl_sync(0xffffffffu, v, 0);
+    if (v >= (unsigned long long)n_work) break;
     process_item<TA, TB>(work[v], work_c[v], ent, d1, d2, out, out_nrm, tbl, cap);
+  }
 }
 
 // Persistent kernel over the global queue of a batch: warps take `grab`
@@ -361,8 +366,12 @@ static int32_t launch_stacked(Ctx* ctx, int64_t n_work, const Work* work, const 
   LAMB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNumWarps * 32, smem));
   const int64_t need = (n_work + kNumWarps - 1) / kNumWarps;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * std::max(per_sm, 1)));
-  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols);
+  unsigned long long* head = nullptr;
+  LAMB_TRY(dalloc(ctx, &head, 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(head, 0, sizeof(unsigned long long), ctx->stream));
+  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols, head);
   LAMB_LAUNCHED(ctx);
+  dfree(ctx, head);
   return LAMB_GPU_OK;
 }
 
