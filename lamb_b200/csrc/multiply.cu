@@ -119,24 +119,18 @@ __device__ __forceinline__ int bm_rank(const uint32_t* bm, const int* wpre, int 
   return wpre[j >> 5] + __popc(bm[j >> 5] & ((1u << (j & 31)) - 1u));
 }
 
-// Fill: the row's A blocks are split into G contiguous k ranges, one per
-// warp (G <= 8).  Each warp counts its entries per C position, the counts are
-// prefix-summed over the warps in k order, and each warp then writes its
-// entries with private cursors.  Entries of one C block therefore come out in
-// k order (warp 0's range first) without a barrier per A block.
 template <bool IDS>
 __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
     const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
-    const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, int32_t max_c, int32_t G,
-    const int64_t* __restrict__ c_row_p, const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col,
-    int64_t* __restrict__ stack_p, const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off,
-    Ent* __restrict__ ent, int2* __restrict__ ids) {
+    const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, const int64_t* __restrict__ c_row_p,
+    const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col, int64_t* __restrict__ stack_p,
+    const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off, Ent* __restrict__ ent,
+    int2* __restrict__ ids) {
   extern __shared__ uint32_t sm[];
   uint32_t* bm = sm;
   int* wpre = (int*)(sm + n_words);
-  int* tot = wpre + n_words;                                   // [max_c]
-  unsigned short* wcnt = (unsigned short*)(tot + max_c + 1);   // [G][max_c]
+  int* cur = wpre + n_words;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kSymThreads / 32;
   for (int64_t i = blockIdx.x; i < n_rows; i += gridDim.x) {
     for (int w = tid; w < n_words; w += kSymThreads) bm[w] = 0u;
@@ -167,57 +161,37 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
         c_col[c0 + p++] = w * 32 + b;
       }
     }
-    for (int t = tid; t < G * nc; t += kSymThreads) wcnt[(t / nc) * max_c + (t % nc)] = 0;
+    for (int t = tid; t < nc; t += kSymThreads) cur[t] = 0;
     __syncthreads();
-    // k range of this warp
-    const int64_t na_blk = a1 - a0;
-    const int64_t per = (na_blk + G - 1) / G;
-    const int64_t r0 = a0 + (int64_t)warp * per, r1 = min(a1, r0 + per);
-    unsigned short* mycnt = wcnt + (size_t)warp * max_c;
-    if (warp < G) {
-      for (int64_t ab = r0; ab < r1; ++ab) {
-        const int k = a_col[ab];
-        const double na = a_nrm[ab];
-        for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
-          if (keep_pair(na, b_nrm[bb], eps, filt)) ++mycnt[bm_rank(bm, wpre, b_col[bb])];
-        __syncwarp();
-      }
+    for (int64_t ab = a0 + warp; ab < a1; ab += nw) {
+      const int k = a_col[ab];
+      const double na = a_nrm[ab];
+      for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
+        if (keep_pair(na, b_nrm[bb], eps, filt)) atomicAdd(&cur[bm_rank(bm, wpre, b_col[bb])], 1);
     }
     __syncthreads();
-    // per position: exclusive prefix over the warps, total into tot[]
-    for (int p = tid; p < nc; p += kSymThreads) {
-      int run = 0;
-      for (int w = 0; w < G; ++w) {
-        const int c = wcnt[(size_t)w * max_c + p];
-        wcnt[(size_t)w * max_c + p] = (unsigned short)run;
-        run += c;
-      }
-      tot[p] = run;
-    }
-    __syncthreads();
-    block_excl_scan_smem(tot, nc);
+    block_excl_scan_smem(cur, nc);
     const int64_t sb = s_row_base[i];
-    for (int t = tid; t < nc; t += kSymThreads) stack_p[c0 + t] = sb + tot[t];
+    for (int t = tid; t < nc; t += kSymThreads) stack_p[c0 + t] = sb + cur[t];
     __syncthreads();
-    if (warp < G) {
-      for (int64_t ab = r0; ab < r1; ++ab) {
-        const int k = a_col[ab];
-        const double na = a_nrm[ab];
-        const long long ak = IDS ? 0 : a_offk[ab];
-        for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
-          if (keep_pair(na, b_nrm[bb], eps, filt)) {
-            const int p = bm_rank(bm, wpre, b_col[bb]);
-            const int64_t slot = sb + tot[p] + mycnt[p];
-            ++mycnt[p];
-            if (IDS)
-              ids[slot] = make_int2((int)ab, (int)bb);
-            else
-              ent[slot] = Ent{ak, (long long)b_off[bb]};
-          }
-        __syncwarp();
-      }
+    // Entries in k order: one A block at a time; the B row's columns are
+    // distinct, so each C position advances at most once per A block.
+    for (int64_t ab = a0; ab < a1; ++ab) {
+      const int k = a_col[ab];
+      const double na = a_nrm[ab];
+      const long long ak = IDS ? 0 : a_offk[ab];
+      for (int64_t bb = b_row_p[k] + tid; bb < b_row_p[k + 1]; bb += kSymThreads)
+        if (keep_pair(na, b_nrm[bb], eps, filt)) {
+          const int p = bm_rank(bm, wpre, b_col[bb]);
+          const int slot = cur[p];
+          cur[p] = slot + 1;
+          if (IDS)
+            ids[sb + slot] = make_int2((int)ab, (int)bb);
+          else
+            ent[sb + slot] = Ent{ak, (long long)b_off[bb]};
+        }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -294,11 +268,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   else
     LAMB_TRY(dalloc(ctx, &out->ent, std::max<int64_t>(out->n_ent, 1)));
   LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
-  // warps splitting a row's k range: as many as the shared memory allows (<= 8)
-  const size_t smem_base = sizeof(uint32_t) * (size_t)std::max(n_words, 1) * 2 + sizeof(int) * (size_t)(max_c + 1);
-  int G = 8;
-  while (G > 1 && smem_base + sizeof(unsigned short) * (size_t)G * (max_c + 1) > 160 * 1024) G >>= 1;
-  const size_t smem_fill = smem_base + sizeof(unsigned short) * (size_t)G * (max_c + 1) + 16;
+  const size_t smem_fill = sizeof(uint32_t) * (size_t)std::max(n_words, 1) * 2 + sizeof(int) * (size_t)(max_c + 1);
   if (smem_fill > 220 * 1024)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
   if (n_rows > 0 && C->nnz > 0) {
@@ -306,8 +276,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     if (smem_fill > 48 * 1024)
       LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
     kern<<<grid, kSymThreads, smem_fill, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms,
-                                                        eps, fl, n_words, (int32_t)(max_c + 1), G, C->row_p,
-                                                        s_row_base, C->col, out->stack_p,
+                                                        eps, fl, n_words, C->row_p, s_row_base, C->col, out->stack_p,
                                                         a_offk, b_meta ? b_meta : B->off, out->ent, out->ids);
     LAMB_LAUNCHED(ctx);
   }
