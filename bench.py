@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-positions", action="store_true", help="order work from the block pattern only")
+    p.add_argument("--mixed-steps", type=int, default=2, help="timed steps of the int8-slice path (0 skips it)")
     return p.parse_args()
 
 
@@ -284,6 +285,21 @@ def run_ours(args):
     alg_bytes = algorithmic_bytes(a, b, c_host)
     peaks, peak_kind = measured_peaks()
     achieved_tf = flops / (ms_num * 1e-3) / 1e12
+    # the int8-slice path on the same inputs, its error taken against the FP64 result
+    mixed = None
+    if args.mixed_steps > 0:
+        dcm = ctx.create_like(da)
+        ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED)
+        mst = [ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED) for _ in range(args.mixed_steps)]
+        ms_m = statistics.mean(s["ms_total"] for s in mst)
+        rel = ctx.diff_frobenius(dcm, dc) / ctx.frobenius(dc)
+        mixed = {"value": flops / (ms_m * 1e-3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms_m,
+                 "ms_numeric": statistics.mean(s["ms_numeric"] for s in mst),
+                 "ms_symbolic": statistics.mean(s["ms_symbolic"] for s in mst),
+                 "slices": int(mst[-1]["mixed_slices"]), "steps": args.mixed_steps,
+                 "rel_frobenius_err_vs_fp64": rel, "ms_ratio_vs_fp64": ms_m / ms_tot,
+                 "path": "int8 digit slices, mma.m16n8k32.s8, exact int32 planes, FP64 recombination"}
+        dcm.destroy()
     # e2e through the C ABI with page-locked host buffers
     pa, pb = pin_matrix(a), pin_matrix(b)
     c_out = dc.download(pinned=True)
@@ -324,10 +340,10 @@ def run_ours(args):
             "config": {"workload": wl.name, "n_mol": wl.n_mol, "n_atoms": g.n_atoms, "box": wl.box,
                        "cutoff": wl.cutoff, "eps": wl.eps, "path": "plain FP64 (DMMA)", "row_order": "pattern (Cuthill-McKee)" if args.no_positions else "Morton (atom coordinates)",
                        "l2": "inputs 2x1.9 GB exceed L2; no flush", "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "tensor", "kernel": "k_numeric_fp64", "achieved": achieved_tf,
+            "roofline": {"bound": "tensor", "kernel": "k_stacked", "achieved": achieved_tf,
                          "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak,
                          "peak_source": "FP64 DMMA probe measured on this GPU in this run",
-                         "traffic": committed_traffic("k_numeric_fp64", wl.name),
+                         "traffic": committed_traffic("k_stacked", wl.name),
                          "flops_per_launch": flops, "ms_per_launch": ms_num},
             "roofline_hbm": {"bound": "hbm", "achieved": alg_bytes / (ms_tot * 1e-3) / 1e9,
                              "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
@@ -338,6 +354,7 @@ def run_ours(args):
                     "ms_per_step": statistics.mean(t_e2e) * 1e3},
             "cpu_baseline": cpu,
             "max_rel_err_vs_oracle": err,
+            "mixed": mixed,
             "stats": {k: stats[-1][k] for k in ("n_products", "n_c_blocks", "ms_symbolic", "ms_numeric", "ms_total")},
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "clocks": clocks,

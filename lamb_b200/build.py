@@ -72,7 +72,8 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
             failed |= p.returncode != 0
         if failed:
             raise RuntimeError("nvcc failed")
-        subprocess.check_call([_nvcc(), "-shared", "-Xcompiler", "-fPIC", "-o", out] + objs + ["-lcudart"],
+        subprocess.check_call([_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler",
+                               "-fPIC", "-o", out] + objs + ["-lcudart"],
                               env=_host_env())
     return out
 

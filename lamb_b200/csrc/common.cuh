@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -40,6 +41,7 @@ struct DevMatrix {
   int32_t* col = nullptr;      // [nnz]
   int64_t* off = nullptr;      // [nnz], 0-based data offset of each block
   double* data = nullptr;      // [data_len]
+  int64_t data_cap = 0;        // elements of data a later multiply into this matrix may reuse (0: none)
   double* norms = nullptr;     // [nnz] Frobenius norms, valid when norms_valid
   bool norms_valid = false;
   // Locality: optional row-atom coordinates (sector order) and the processing
@@ -50,6 +52,9 @@ struct DevMatrix {
   int32_t* order = nullptr;      // device copy of h_order
 };
 
+// Roles of the context's grow-only scratch buffers (multiply temporaries).
+enum ScratchSlot : int { kScrEnt = 0, kScrWork, kScrWorkC, kScrPlaneA, kScrPlaneB, kScrSlots };
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -59,7 +64,18 @@ struct Ctx {
   lamb_gpu_mult_stats last_stats{};
   int64_t launches = 0;  // kernels of this library launched on the context
   cudaEvent_t ev[8] = {};
+  bool trace = false;     // LAMB_GPU_TRACE=1 at creation: phase timings on stderr
+  double trace_t = 0.0;   // host time of the previous trace mark (ms)
+  // Multiply temporaries of several GB (stacks, work items, digit planes) are
+  // kept between calls: releasing and re-reserving them fragments the
+  // stream-ordered pool, which then maps fresh memory at up to a second a call.
+  void* scr[kScrSlots] = {};
+  size_t scr_bytes[kScrSlots] = {};
 };
+
+// With tracing on, waits for the stream and prints the host time since the
+// previous mark; otherwise does nothing.
+void trace_mark(Ctx* ctx, const char* what);
 
 // Error helpers: set the message, return the encoded status.
 int32_t fail(Ctx* ctx, int level, int type, const std::string& msg);
@@ -77,20 +93,26 @@ int32_t fail(Ctx* ctx, int level, int type, const std::string& msg);
     if (st_ != LAMB_GPU_OK) return st_; \
   } while (0)
 
-// Stream-ordered allocation on the context's stream.
+// Stream-ordered allocation on the context's stream.  When the pool cannot
+// satisfy a request, unused pool memory is returned to the device once and the
+// allocation retried.
+int32_t dalloc_bytes(Ctx* ctx, void** p, size_t bytes);
 template <typename T>
 int32_t dalloc(Ctx* ctx, T** p, int64_t n) {
   *p = nullptr;
   if (n <= 0) return LAMB_GPU_OK;
-  cudaError_t e = cudaMallocAsync((void**)p, sizeof(T) * (size_t)n, ctx->stream);
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return fail(ctx, LAMB_LEVEL_MEMORY, LAMB_TYPE_EXTERNAL_ERROR,
-                std::string("device allocation of ") + std::to_string(sizeof(T) * (size_t)n) +
-                    " bytes failed: " + cudaGetErrorString(e));
-  }
-  return LAMB_GPU_OK;
+  return dalloc_bytes(ctx, reinterpret_cast<void**>(p), sizeof(T) * (size_t)n);
 }
+
+// Grow-only scratch buffer of the context for one role; the contents do not
+// survive the next call that uses the same role.
+int32_t scratch_bytes(Ctx* ctx, int slot, size_t bytes, void** p);
+template <typename T>
+int32_t scratch(Ctx* ctx, int slot, int64_t n, T** p) {
+  return scratch_bytes(ctx, slot, sizeof(T) * (size_t)std::max<int64_t>(n, 1), reinterpret_cast<void**>(p));
+}
+void release_scratch(Ctx* ctx);
+
 template <typename T>
 void dfree(Ctx* ctx, T*& p) {
   if (p) cudaFreeAsync((void*)p, ctx->stream);

@@ -9,6 +9,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 
 #include "common.cuh"
 
@@ -17,6 +20,59 @@ namespace lamb {
 int32_t fail(Ctx* ctx, int level, int type, const std::string& msg) {
   if (ctx) ctx->last_error = msg;
   return make_status(level, type);
+}
+
+int32_t dalloc_bytes(Ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cudaMemPool_t pool;
+    if (cudaStreamSynchronize(ctx->stream) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess &&
+        cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+      e = cudaMallocAsync(p, bytes, ctx->stream);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(ctx, LAMB_LEVEL_MEMORY, LAMB_TYPE_EXTERNAL_ERROR,
+                "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  return LAMB_GPU_OK;
+}
+
+int32_t scratch_bytes(Ctx* ctx, int slot, size_t bytes, void** p) {
+  if (bytes > ctx->scr_bytes[slot]) {
+    if (ctx->scr[slot]) cudaFreeAsync(ctx->scr[slot], ctx->stream);
+    ctx->scr[slot] = nullptr;
+    ctx->scr_bytes[slot] = 0;
+    const size_t mib2 = size_t(2) << 20;
+    size_t want = ((bytes + bytes / 16) + mib2 - 1) / mib2 * mib2;  // headroom for the next, slightly larger call
+    if (dalloc_bytes(ctx, &ctx->scr[slot], want) != LAMB_GPU_OK) {
+      want = bytes;
+      LAMB_TRY(dalloc_bytes(ctx, &ctx->scr[slot], want));
+    }
+    ctx->scr_bytes[slot] = want;
+  }
+  *p = ctx->scr[slot];
+  return LAMB_GPU_OK;
+}
+
+void release_scratch(Ctx* ctx) {
+  for (int i = 0; i < kScrSlots; ++i) {
+    if (ctx->scr[i]) cudaFreeAsync(ctx->scr[i], ctx->stream);
+    ctx->scr[i] = nullptr;
+    ctx->scr_bytes[i] = 0;
+  }
+}
+
+void trace_mark(Ctx* ctx, const char* what) {
+  if (!ctx->trace) return;
+  cudaStreamSynchronize(ctx->stream);
+  const double now =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  std::fprintf(stderr, "[lamb trace] %-28s %10.2f ms\n", what, ctx->trace_t > 0 ? now - ctx->trace_t : 0.0);
+  ctx->trace_t = now;
 }
 
 DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h) {
@@ -31,6 +87,7 @@ void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
   dfree(ctx, m->col);
   dfree(ctx, m->off);
   dfree(ctx, m->data);
+  m->data_cap = 0;
   dfree(ctx, m->norms);
   dfree(ctx, m->order);
   m->h_order.clear();
@@ -413,6 +470,7 @@ int32_t lamb_gpu_ctx_create(int32_t device, lamb_gpu_ctx** out) {
     return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+  if (const char* t = std::getenv("LAMB_GPU_TRACE")) ctx->trace = t[0] == '1';
   // Keep freed stream-ordered memory in the pool between calls.
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -429,6 +487,7 @@ int32_t lamb_gpu_ctx_destroy(lamb_gpu_ctx* c) {
   cudaSetDevice(ctx->device);
   for (auto& kv : ctx->mats) free_matrix_buffers(ctx, kv.second.get());
   ctx->mats.clear();
+  release_scratch(ctx);
   cudaStreamSynchronize(ctx->stream);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
   cudaStreamDestroy(ctx->stream);

@@ -40,37 +40,50 @@ constexpr int kMaxSlices = 8;
 __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
 // ---- scales ----------------------------------------------------------------------------
-// Row exponents of A: one warp per block row, one lane per element row.
+// Row exponents of A: one warp per block row; lanes take whole blocks and
+// merge their per-row maxima with shared-memory atomics (non-negative doubles
+// order like their bit patterns).
 __global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                           const int8_t* __restrict__ col_bs, const double* __restrict__ d,
                           const int64_t* __restrict__ ebase, int* __restrict__ ea) {
-  const int lane = threadIdx.x & 31;
+  __shared__ unsigned long long pm[8][128];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
     const int bi = row_bs[r];
-    for (int p = lane; p < bi; p += 32) {
-      double m = 0.0;
-      for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-        const int bk = col_bs[col[b]];
-        const double* x = d + off[b];
+    for (int p = lane; p < bi; p += 32) pm[wl][p] = 0ull;
+    __syncwarp();
+    for (int64_t b = row_p[r] + lane; b < row_p[r + 1]; b += 32) {
+      const int bk = col_bs[col[b]];
+      const double* x = d + off[b];
+      for (int p = 0; p < bi; ++p) {
+        double m = 0.0;
         for (int q = 0; q < bk; ++q) m = fmax(m, fabs(x[(int64_t)q * bi + p]));
+        atomicMax(&pm[wl][p], (unsigned long long)__double_as_longlong(m));
       }
+    }
+    __syncwarp();
+    for (int p = lane; p < bi; p += 32) {
       int e = 0;
-      frexp(m, &e);
+      frexp(__longlong_as_double((long long)pm[wl][p]), &e);
       ea[ebase[r] + p] = e;
     }
+    __syncwarp();
   }
 }
 
-// Column exponents of B: one thread per block, atomic max per element column.
+// Column exponents of B: one warp per block row, lanes over its blocks, one
+// global atomic max per block column element.
 __global__ void k_col_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                           const int8_t* __restrict__ col_bs, const double* __restrict__ d,
                           const int64_t* __restrict__ ebase, int* __restrict__ eb) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
     const int bk = row_bs[r];
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+    for (int64_t b = row_p[r] + lane; b < row_p[r + 1]; b += 32) {
       const int j = col[b], bj = col_bs[j];
       const double* x = d + off[b];
       for (int c = 0; c < bj; ++c) {
@@ -381,6 +394,7 @@ static std::vector<int64_t> elem_base(const std::vector<int8_t>& bs) {
 int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp) {
   if (max_block(A->h_row_bs) > 127 || max_block(B->h_col_bs) > 127)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "mixed: block too large");
+  static_assert(kThreads <= 256, "k_row_exp keeps 8 warps x 128 rows of maxima in shared memory");
   mp->s = s;
   const auto ra = elem_base(A->h_row_bs), cbv = elem_base(B->h_col_bs);
   LAMB_TRY(dalloc(ctx, &mp->rbase, (int64_t)ra.size()));
@@ -397,10 +411,11 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
     LAMB_LAUNCHED(ctx);
   }
   if (B->nnz) {
-    k_col_exp<<<grid_for(B->n_rows, 128), 128, 0, ctx->stream>>>(B->n_rows, B->row_p, B->col, B->off, B->row_bs,
-                                                                   B->col_bs, B->data, mp->cbase, mp->eb);
+    k_col_exp<<<grid_for((int64_t)B->n_rows * 32), kThreads, 0, ctx->stream>>>(
+        B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, mp->cbase, mp->eb);
     LAMB_LAUNCHED(ctx);
   }
+  trace_mark(ctx, "slice exponents");
   // plane offsets
   int64_t* sz = nullptr;
   LAMB_TRY(dalloc(ctx, &mp->a_soff, std::max<int64_t>(A->nnz, 1) + 1));
@@ -422,8 +437,9 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
   LAMB_TRY(plane(A, 1, mp->a_soff, &mp->a_plane));
   LAMB_TRY(plane(B, 0, mp->b_soff, &mp->b_plane));
   dfree(ctx, sz);
-  LAMB_TRY(dalloc(ctx, &mp->a_planes, mp->a_plane * s));
-  LAMB_TRY(dalloc(ctx, &mp->b_planes, mp->b_plane * s));
+  trace_mark(ctx, "plane sizes");
+  LAMB_TRY(scratch(ctx, kScrPlaneA, mp->a_plane * s, &mp->a_planes));
+  LAMB_TRY(scratch(ctx, kScrPlaneB, mp->b_plane * s, &mp->b_planes));
   if (A->nnz) {
     k_digits<<<grid_for((int64_t)A->n_rows * 32), kThreads, 0, ctx->stream>>>(
         A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, mp->rbase, nullptr, mp->ea, nullptr, 1,
@@ -441,7 +457,8 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
 
 void free_slices(Ctx* ctx, MixedPlanes* mp) {
   dfree(ctx, mp->rbase); dfree(ctx, mp->cbase); dfree(ctx, mp->ea); dfree(ctx, mp->eb);
-  dfree(ctx, mp->a_soff); dfree(ctx, mp->b_soff); dfree(ctx, mp->a_planes); dfree(ctx, mp->b_planes);
+  dfree(ctx, mp->a_soff); dfree(ctx, mp->b_soff);
+  mp->a_planes = mp->b_planes = nullptr;  // context scratch
 }
 
 // (plane offset | inner size << 56) for every A block; plane offsets of B.

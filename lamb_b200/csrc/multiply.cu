@@ -19,7 +19,10 @@ namespace lamb {
 
 void free_symbolic(Ctx* ctx, Symbolic& s) {
   dfree(ctx, s.stack_p);
-  dfree(ctx, s.ent);
+  if (s.use_scratch)
+    s.ent = nullptr;
+  else
+    dfree(ctx, s.ent);
   dfree(ctx, s.ids);
   dfree(ctx, s.c_row);
 }
@@ -202,14 +205,24 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_TRY(check_compatible(ctx, A, B));
   LAMB_TRY(ensure_norms(ctx, A));
   LAMB_TRY(ensure_norms(ctx, B));
+  trace_mark(ctx, "operand norms");
   if (A->nnz >= (1ll << 31) || B->nnz >= (1ll << 31))
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "more than 2^31 blocks in an operand");
   if (!want_ids && !a_offk) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "symbolic: no A meta");
-  // C takes A's row subsets and B's column subsets.
+  // C takes A's row subsets and B's column subsets.  Its data buffer is kept
+  // for the new pattern when large enough (freed on every early return).
+  struct KeptData {
+    Ctx* ctx;
+    double* p;
+    int64_t cap;
+    ~KeptData() { dfree(ctx, p); }
+  } kept{ctx, C->data, C->data_cap};
+  C->data = nullptr;
   free_matrix_buffers(ctx, C);
   copy_structure(C, A, true, B, true);
   LAMB_TRY(inherit_row_locality(ctx, C, A));
   LAMB_TRY(upload_block_sizes(ctx, C));
+  trace_mark(ctx, "C structure");
   const int32_t n_rows = C->n_rows;
   const int32_t n_words = (C->n_cols + 31) / 32;
   LAMB_TRY(dalloc(ctx, &C->row_p, n_rows + 1));
@@ -242,6 +255,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_f.data(), rfl, sizeof(double) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  trace_mark(ctx, "symbolic count");
   std::vector<int64_t> h_crp(n_rows + 1, 0), h_srb(n_rows + 1, 0);
   int64_t max_c = 0, max_s = 0;
   for (int r = 0; r < n_rows; ++r) {
@@ -265,9 +279,12 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_TRY(dalloc(ctx, &out->stack_p, C->nnz + 1));
   if (want_ids)
     LAMB_TRY(dalloc(ctx, &out->ids, std::max<int64_t>(out->n_ent, 1)));
+  else if (out->use_scratch)
+    LAMB_TRY(scratch(ctx, kScrEnt, out->n_ent, &out->ent));
   else
     LAMB_TRY(dalloc(ctx, &out->ent, std::max<int64_t>(out->n_ent, 1)));
   LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+  trace_mark(ctx, "symbolic allocations");
   const size_t smem_fill = sizeof(uint32_t) * (size_t)std::max(n_words, 1) * 2 + sizeof(int) * (size_t)(max_c + 1);
   if (smem_fill > 220 * 1024)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
@@ -280,11 +297,23 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
                                                         a_offk, b_meta ? b_meta : B->off, out->ent, out->ids);
     LAMB_LAUNCHED(ctx);
   }
+  trace_mark(ctx, "symbolic fill");
   LAMB_TRY(dalloc(ctx, &out->c_row, std::max<int64_t>(C->nnz, 1)));
   LAMB_TRY(layout_sector_major(ctx, C, out->c_row));
+  trace_mark(ctx, "sector layout");
   if (C->data_len >= kMask40) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C data too large");
-  LAMB_TRY(dalloc(ctx, &C->data, std::max<int64_t>(C->data_len, 1)));
+  const int64_t need = std::max<int64_t>(C->data_len, 1);
+  if (kept.p && kept.cap >= need) {
+    C->data = kept.p;
+    C->data_cap = kept.cap;
+    kept.p = nullptr;
+  } else {
+    dfree(ctx, kept.p);
+    LAMB_TRY(dalloc(ctx, &C->data, need));
+    C->data_cap = need;
+  }
   dfree(ctx, c_cnt); dfree(ctx, s_cnt); dfree(ctx, p_cnt); dfree(ctx, rfl); dfree(ctx, s_row_base);
+  trace_mark(ctx, "C data allocation");
   return LAMB_GPU_OK;
 }
 
@@ -328,10 +357,15 @@ __global__ void k_build_work(int32_t n_rows, const int32_t* __restrict__ order, 
 }
 
 int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
-                   int32_t** work_c) {
+                   int32_t** work_c, bool use_scratch) {
   const int n = C->n_rows;
-  LAMB_TRY(dalloc(ctx, work, std::max<int64_t>(sym.c_nnz, 1)));
-  LAMB_TRY(dalloc(ctx, work_c, std::max<int64_t>(sym.c_nnz, 1)));
+  if (use_scratch) {
+    LAMB_TRY(scratch(ctx, kScrWork, sym.c_nnz, work));
+    LAMB_TRY(scratch(ctx, kScrWorkC, sym.c_nnz, work_c));
+  } else {
+    LAMB_TRY(dalloc(ctx, work, std::max<int64_t>(sym.c_nnz, 1)));
+    LAMB_TRY(dalloc(ctx, work_c, std::max<int64_t>(sym.c_nnz, 1)));
+  }
   if (sym.c_nnz == 0 || n == 0) return LAMB_GPU_OK;
   if ((int)order_src->h_order.size() != n || !order_src->order)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "work list: row order missing");
@@ -446,28 +480,36 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   int64_t dropped = 0;
   MixedPlanes mp;
   const bool mixed = (flags & LAMB_GPU_MIXED) != 0;
+  sym.use_scratch = true;
   auto body = [&]() -> int32_t {
+    trace_mark(ctx, "multiply: start");
     LAMB_TRY(check_compatible(ctx, A, B));
     LAMB_TRY(ensure_row_order(ctx, A));
+    trace_mark(ctx, "row order");
     if (mixed) {
       slices = mixed_slices_from_env();
       LAMB_TRY(build_slices(ctx, A, B, slices, &mp));
+      trace_mark(ctx, "digit slices");
       LAMB_TRY(pack_plane_meta(ctx, A, mp, &a_offk));
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym, mp.b_soff));
     } else {
       LAMB_TRY(pack_offk(ctx, A, true, &a_offk));
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
     }
-    LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c));
+    trace_mark(ctx, "symbolic");
+    LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c, true));
     LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
+    trace_mark(ctx, "work items");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     if (mixed)
       LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, mp));
     else
       LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false,
                               max_block(A->h_col_bs)));
+    trace_mark(ctx, "numeric");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps, &dropped));
+    trace_mark(ctx, "result filter");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
     return LAMB_GPU_OK;
   };
@@ -475,8 +517,6 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   free_slices(ctx, &mp);
   dfree(ctx, a_offk);
   dfree(ctx, c_nrm);
-  dfree(ctx, work);
-  dfree(ctx, work_c);
   free_symbolic(ctx, sym);
   if (rc != LAMB_GPU_OK) return rc;
   C->norms_valid = false;

@@ -38,6 +38,7 @@ struct Symbolic {
   int2* ids = nullptr;         // [n_ent] when ids were requested
   int32_t* c_row = nullptr;    // [c_nnz] row of every C block
   std::vector<int64_t> h_row_len;  // C blocks per row (host)
+  bool use_scratch = false;    // set before symbolic_phase: ent lives in the context's scratch
 };
 void free_symbolic(Ctx* ctx, Symbolic& s);
 
@@ -50,8 +51,9 @@ int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk);
 int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, bool want_ids,
                        const int64_t* a_offk, Symbolic* out, const int64_t* b_meta = nullptr);
 // Work list of C blocks in the row processing order of `order_src` (its h_order).
+// use_scratch: work and work_c come from the context's scratch (not to be freed).
 int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
-                   int32_t** work_c);
+                   int32_t** work_c, bool use_scratch = false);
 // Stacked small-GEMM kernels: out_c = sum_e op1_e . op2_e over the work list.
 // TA/TB select transposed operands (used by the adjoint); see numeric.cu.
 // max_inner: the largest inner block size of any entry (sizes the column table).
