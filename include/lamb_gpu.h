@@ -175,6 +175,55 @@ LAMB_API int32_t lamb_gpu_matrix_destroy(lamb_gpu_ctx* ctx, lamb_gpu_matrix hand
  * on the order. */
 LAMB_API int32_t lamb_gpu_matrix_set_positions(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, const float* xyz,
                                                int32_t n_rows, const float* box);
+/* Builds a device matrix from a coordinate block list (host arrays): block b
+ * sits at global atoms (blk_row[b], blk_col[b]) (1-based) and its
+ * column-major elements at data[extents[2b]-1 .. extents[2b+1]-1] (1-based,
+ * inclusive; the extent length must equal the block size).  Every atom names
+ * its subset (1-based); local atoms follow global order inside a subset.
+ * Replaces, on the GPU, lamb_dist_localize_index + internal_distribute at one
+ * rank + fill_local_sectors + lamb_index_convert_to_csr
+ * (src/lamb_matrix_operations.F90:88-371, src/lamb_index_methods.F90:224-246);
+ * blocks may come in any order (they are sorted on the device), duplicates
+ * are an error. */
+LAMB_API int32_t lamb_gpu_matrix_from_coo(lamb_gpu_ctx* ctx, int32_t n_atom_rows, int32_t n_atom_cols,
+                                          const int8_t* row_blk_sizes, const int8_t* col_blk_sizes,
+                                          const int32_t* row_subset, const int32_t* col_subset, int64_t n_blks,
+                                          const int32_t* blk_row, const int32_t* blk_col, const int64_t* extents,
+                                          const double* data, int64_t data_len, lamb_gpu_matrix* handle);
+
+/* DBCSR dump files (the format lamb_load_dbcsr reads,
+ * src/lamb_io_operations.F90:267-756).  Host-only; no device needed. */
+typedef struct lamb_dbcsr_info {
+  char name[81];         /* matrix name (sub-header 1), trailing blanks removed */
+  char matrix_type;      /* 'N' (no symmetry), 'S', 'A', 'H', 'K'             */
+  int32_t n_chunks;      /* numnodes: chunks (one per writing process)         */
+  int32_t data_type;     /* DBCSR data type code as stored                     */
+  int32_t n_block_rows;  /* nblkrows_total                                     */
+  int32_t n_block_cols;  /* nblkcols_total                                     */
+  int64_t n_blks;        /* blocks over all chunks                             */
+  int64_t data_len;      /* doubles read: per chunk up to its largest extent   */
+} lamb_dbcsr_info;
+/* Sizes of a dump (size phase of the size->fill protocol); on failure
+ * msg[msg_len] gets the reason. */
+LAMB_API int32_t lamb_dbcsr_scan(const char* path, lamb_dbcsr_info* info, char* msg, int32_t msg_len);
+/* The dump's blocks in coordinate form (load_dbcsr_chunks,
+ * src/lamb_io_operations.F90:525-700): block sizes [n_block_rows] and
+ * [n_block_cols], rows/cols [n_blks] (1-based global atoms, chunk after
+ * chunk, CSR order inside a chunk), extents [2*n_blks] (1-based, inclusive)
+ * into data, the chunks' data areas concatenated (data_cap >= data_len). */
+LAMB_API int32_t lamb_dbcsr_read(const char* path, int32_t* row_blk_size, int32_t* col_blk_size, int32_t* rows,
+                                 int32_t* cols, int64_t* extents, double* data, int64_t data_cap, char* msg,
+                                 int32_t msg_len);
+/* lamb_load_dbcsr at one rank: reads a dump ('N' matrices) and builds the
+ * device matrix through lamb_gpu_matrix_from_coo.  Atoms are split into
+ * n_x_cubes subsets along x by the single-rank partition rule
+ * 1 + mod(int(x * (n_x_cubes / h11)), n_x_cubes) in single precision, with
+ * h11 the largest x of the coordinates (xyz[3*n_block_rows], the contents of
+ * the reference's coordinate file; columns take the row atoms'
+ * coordinates); n_x_cubes = 1 puts every atom in subset 1 and needs no
+ * coordinates. */
+LAMB_API int32_t lamb_gpu_matrix_load_dbcsr(lamb_gpu_ctx* ctx, const char* path, const float* xyz,
+                                            int32_t n_x_cubes, lamb_gpu_matrix* handle);
 /* Number of sectors, then per-sector sizes (sizes[n_sectors]). */
 LAMB_API int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, int32_t* n_sectors);
 LAMB_API int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_sizes* sizes,

@@ -49,6 +49,19 @@ class PurifyReport(C.Structure):
     ]
 
 
+class DbcsrInfo(C.Structure):
+    """lamb_dbcsr_info (include/lamb_gpu.h)."""
+    _fields_ = [("name", C.c_char * 81), ("matrix_type", C.c_char), ("n_chunks", C.c_int32),
+                ("data_type", C.c_int32), ("n_block_rows", C.c_int32), ("n_block_cols", C.c_int32),
+                ("n_blks", C.c_int64), ("data_len", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["name"] = d["name"].decode("ascii", "replace")
+        d["matrix_type"] = d["matrix_type"].decode("ascii", "replace")
+        return d
+
+
 def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data if a is not None and a.size else 0
 

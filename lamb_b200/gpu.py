@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from .abi import CSector, CSectorOut, CSectorSizes, MultStats, PurifyReport, sector_to_c
+from .abi import CSector, CSectorOut, CSectorSizes, DbcsrInfo, MultStats, PurifyReport, sector_to_c
 from .matrix import LambMatrix, Sector
 
 FP64 = 0
@@ -59,6 +59,10 @@ def lib() -> C.CDLL:
             "lamb_gpu_ctx_get_stream": [vp, P(vp)],
             "lamb_gpu_ctx_synchronize": [vp],
             "lamb_gpu_matrix_upload": [vp, P(CSector), i32, P(i64)],
+            "lamb_gpu_matrix_from_coo": [vp, i32, i32, vp, vp, vp, vp, i64, vp, vp, vp, vp, i64, P(i64)],
+            "lamb_gpu_matrix_load_dbcsr": [vp, C.c_char_p, vp, i32, P(i64)],
+            "lamb_dbcsr_scan": [C.c_char_p, P(DbcsrInfo), C.c_char_p, i32],
+            "lamb_dbcsr_read": [C.c_char_p, vp, vp, vp, vp, vp, vp, i64, C.c_char_p, i32],
             "lamb_gpu_matrix_create_like": [vp, i64, P(i64)],
             "lamb_gpu_matrix_destroy": [vp, i64],
             "lamb_gpu_matrix_n_sectors": [vp, i64, P(i32)],
@@ -89,6 +93,32 @@ def lib() -> C.CDLL:
             f.restype = i32
         _typed = True
     return L
+
+
+def dbcsr_scan(path: str) -> dict:
+    """Sizes and header fields of a DBCSR dump (lamb_dbcsr_scan; host only)."""
+    info, msg = DbcsrInfo(), C.create_string_buffer(512)
+    st = lib().lamb_dbcsr_scan(path.encode(), C.byref(info), msg, 512)
+    if st != 0:
+        raise LambError(st, msg.value.decode(errors="replace"))
+    return info.as_dict()
+
+
+def dbcsr_read(path: str) -> dict:
+    """A DBCSR dump's blocks in coordinate form (lamb_dbcsr_read; host only)."""
+    info = dbcsr_scan(path)
+    rbs = np.zeros(info["n_block_rows"], np.int32)
+    cbs = np.zeros(info["n_block_cols"], np.int32)
+    rows = np.zeros(info["n_blks"], np.int32)
+    cols = np.zeros(info["n_blks"], np.int32)
+    ext = np.zeros((info["n_blks"], 2), np.int64)
+    data = np.zeros(info["data_len"], np.float64)
+    msg = C.create_string_buffer(512)
+    st = lib().lamb_dbcsr_read(path.encode(), rbs.ctypes.data, cbs.ctypes.data, rows.ctypes.data, cols.ctypes.data,
+                               ext.ctypes.data, data.ctypes.data, data.size, msg, 512)
+    if st != 0:
+        raise LambError(st, msg.value.decode(errors="replace"))
+    return dict(info=info, row_blk_size=rbs, col_blk_size=cbs, rows=rows, cols=cols, extents=ext, data=data)
 
 
 class Context:
@@ -135,6 +165,33 @@ class Context:
         arr = (CSector * len(m.sectors))(*[sector_to_c(s) for s in m.sectors])
         h = C.c_int64()
         self.check(lib().lamb_gpu_matrix_upload(self._h, arr, len(m.sectors), C.byref(h)))
+        return DeviceMatrix(self, h.value)
+
+    def from_coo(self, row_blk_sizes, col_blk_sizes, row_subset, col_subset, blk_row, blk_col, extents,
+                 data) -> "DeviceMatrix":
+        """Device matrix from a coordinate block list (lamb_gpu_matrix_from_coo):
+        1-based global atoms per block, 1-based inclusive extents into data."""
+        rbs = np.ascontiguousarray(row_blk_sizes, np.int8)
+        cbs = np.ascontiguousarray(col_blk_sizes, np.int8)
+        rs = np.ascontiguousarray(row_subset, np.int32)
+        cs = np.ascontiguousarray(col_subset, np.int32)
+        br = np.ascontiguousarray(blk_row, np.int32)
+        bc = np.ascontiguousarray(blk_col, np.int32)
+        ex = np.ascontiguousarray(extents, np.int64).reshape(-1)
+        d = np.ascontiguousarray(data, np.float64)
+        h = C.c_int64()
+        self.check(lib().lamb_gpu_matrix_from_coo(self._h, rbs.size, cbs.size, rbs.ctypes.data, cbs.ctypes.data,
+                                                  rs.ctypes.data, cs.ctypes.data, br.size, br.ctypes.data,
+                                                  bc.ctypes.data, ex.ctypes.data, d.ctypes.data, d.size,
+                                                  C.byref(h)))
+        return DeviceMatrix(self, h.value)
+
+    def load_dbcsr(self, path: str, xyz: Optional[np.ndarray] = None, n_x_cubes: int = 1) -> "DeviceMatrix":
+        """lamb_load_dbcsr at one rank (lamb_gpu_matrix_load_dbcsr)."""
+        x = None if xyz is None else np.ascontiguousarray(xyz, np.float32).reshape(-1)
+        h = C.c_int64()
+        self.check(lib().lamb_gpu_matrix_load_dbcsr(self._h, path.encode(), None if x is None else x.ctypes.data,
+                                                    n_x_cubes, C.byref(h)))
         return DeviceMatrix(self, h.value)
 
     def create_like(self, like: "DeviceMatrix") -> "DeviceMatrix":
