@@ -293,7 +293,18 @@ def run_ours(args):
         mst = [ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED) for _ in range(args.mixed_steps)]
         ms_m = statistics.mean(s["ms_total"] for s in mst)
         rel = ctx.diff_frobenius(dcm, dc) / ctx.frobenius(dc)
+        lib.lamb_probe_int8_tops.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+        ipeak = ctypes.c_double()
+        ctx.check(lib.lamb_probe_int8_tops(local, 5, ctypes.byref(ipeak)))
+        s_m = int(mst[-1]["mixed_slices"])
+        ms_mn = statistics.mean(s["ms_numeric"] for s in mst)
+        # every FP64-equivalent flop is s(s+1)/2 int8 plane-product ops (digit pairs p + q <= s - 1)
+        int8_tops = flops * (s_m * (s_m + 1) // 2) / (ms_mn * 1e-3) / 1e12
         mixed = {"value": flops / (ms_m * 1e-3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms_m,
+                 "roofline": {"bound": "tensor", "kernel": "k_mixed", "achieved": int8_tops, "peak": ipeak.value,
+                              "unit": "TOP/s (int8)", "frac": int8_tops / ipeak.value,
+                              "peak_source": "mma.m16n8k32.s8 probe measured on this GPU in this run",
+                              "ops": "FP64-equivalent flops x s(s+1)/2 digit-pair products"},
                  "ms_numeric": statistics.mean(s["ms_numeric"] for s in mst),
                  "ms_symbolic": statistics.mean(s["ms_symbolic"] for s in mst),
                  "slices": int(mst[-1]["mixed_slices"]), "steps": args.mixed_steps,
@@ -308,7 +319,8 @@ def run_ours(args):
     d2h = matrix_bytes(c_out)
     barrier()
     t_e2e = []
-    for _ in range(max(1, args.e2e_steps)):
+    # one untimed pass first: the device memory pool grows to the working set
+    for it in range(1 + max(1, args.e2e_steps)):
         torch.cuda.synchronize()
         t = time.perf_counter()
         xa, xb = ctx.upload(pa), ctx.upload(pb)
@@ -318,7 +330,8 @@ def run_ours(args):
         st_e = ctx.multiply(xa, xb, xc, wl.eps)
         c_out = xc.download(out=c_out)
         xc.destroy(); xb.destroy(); xa.destroy()
-        t_e2e.append(time.perf_counter() - t)
+        if it > 0:
+            t_e2e.append(time.perf_counter() - t)
     e2e_t = torch.tensor([statistics.mean(t_e2e)], device="cuda")
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)

@@ -1,7 +1,7 @@
 /*
  * lamb_probe.h -- measurement helper of liblamb_b200.so (not part of the
- * drop-in ABI): the FP64 tensor-pipe peak of the current GPU, used as the
- * roofline denominator of the FP64 multiply.  No reference counterpart.
+ * drop-in ABI): the FP64 and int8 tensor-pipe peaks of the current GPU, used
+ * as the roofline denominators of the FP64 and the int8-slice multiplies.  No reference counterpart.
  */
 #ifndef LAMB_PROBE_H
 #define LAMB_PROBE_H
@@ -13,6 +13,10 @@ extern "C" {
 /* Best of `reps` launches of a DMMA (mma.m8n8k4.f64) throughput loop on
  * `device`; writes TFLOP/s.  Allocates 8 bytes per thread of the grid. */
 LAMB_API int32_t lamb_probe_fp64_tflops(int32_t device, int32_t reps, double* tflops);
+/* Same for the integer tensor pipe as the int8-slice kernel drives it
+ * (mma.m16n8k32.s8.s8.s32 through mma.sync); writes TOP/s (1 op = 1 multiply
+ * or 1 add).  Allocates 4 bytes per thread of the grid. */
+LAMB_API int32_t lamb_probe_int8_tops(int32_t device, int32_t reps, double* tops);
 #ifdef __cplusplus
 }
 #endif

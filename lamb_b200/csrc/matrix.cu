@@ -261,6 +261,37 @@ __global__ void k_part_offsets(int32_t n_rows, int32_t n_rsub, int32_t S, const 
   }
 }
 
+// Sector index of every block for downloads: position bpos[idx(m,n,l)] + i
+// of the i-th block of local row l in sector (m,n) in an array ordered sector
+// by sector; column 1-based within the column subset, extents 1-based
+// inclusive within the sector's data.
+__global__ void k_sector_index(int32_t n_rows, int32_t n_rsub, int32_t S, const int32_t* __restrict__ rsub_base,
+                               const int32_t* __restrict__ csub_base, const int64_t* __restrict__ row_p,
+                               const int32_t* __restrict__ col, const int64_t* __restrict__ off,
+                               const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs,
+                               const int64_t* __restrict__ bpos, const int64_t* __restrict__ sec_base,
+                               int16_t* __restrict__ col16, int64_t* __restrict__ ext) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int m = 0;
+    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+    const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
+    const int64_t l = r - rsub_base[m];
+    const int64_t base = (int64_t)rsub_base[m] * S + l;
+    const int64_t bi = row_bs[r];
+    int n = 0;
+    int64_t q = bpos[base];
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      const int c = col[b];
+      while (c >= csub_base[n + 1]) { ++n; q = bpos[base + n * cnt]; }
+      const int64_t e1 = off[b] - sec_base[(int64_t)m * S + n] + 1;
+      col16[q] = (int16_t)(c - csub_base[n] + 1);
+      ext[2 * q] = e1;
+      ext[2 * q + 1] = e1 + bi * col_bs[c] - 1;
+      ++q;
+    }
+  }
+}
+
 int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of) {
   const int S = m->n_csub;
   const int64_t n_seq = (int64_t)m->n_rows * S;
@@ -581,6 +612,12 @@ int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_
   }
   m->data_len = dpos;
   m->nnz = nnz;
+  // Block data first: the copies run while the index is built on the host.
+  LAMB_TRY(dalloc(ctx, &m->data, std::max<int64_t>(m->data_len, 1)));
+  for (size_t k = 0; k < sid.size(); ++k)
+    if (sid[k] >= 0 && sec[sid[k]].data_len > 0)
+      LAMB_CUDA(ctx, cudaMemcpyAsync(m->data + m->sec_base[k], sec[sid[k]].data, sizeof(double) * sec[sid[k]].data_len,
+                                     cudaMemcpyHostToDevice, ctx->stream));
   std::vector<int64_t> h_row_p(m->n_rows + 1, 0), h_off(nnz);
   std::vector<int32_t> h_col(nnz);
   int64_t p = 0;
@@ -603,16 +640,11 @@ int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_
   LAMB_TRY(dalloc(ctx, &m->row_p, m->n_rows + 1));
   LAMB_TRY(dalloc(ctx, &m->col, std::max<int64_t>(nnz, 1)));
   LAMB_TRY(dalloc(ctx, &m->off, std::max<int64_t>(nnz, 1)));
-  LAMB_TRY(dalloc(ctx, &m->data, std::max<int64_t>(m->data_len, 1)));
   LAMB_CUDA(ctx, cudaMemcpyAsync(m->row_p, h_row_p.data(), sizeof(int64_t) * (m->n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
   if (nnz) {
     LAMB_CUDA(ctx, cudaMemcpyAsync(m->col, h_col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(m->off, h_off.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
   }
-  for (size_t k = 0; k < sid.size(); ++k)
-    if (sid[k] >= 0 && sec[sid[k]].data_len > 0)
-      LAMB_CUDA(ctx, cudaMemcpyAsync(m->data + m->sec_base[k], sec[sid[k]].data, sizeof(double) * sec[sid[k]].data_len,
-                                     cudaMemcpyHostToDevice, ctx->stream));
   // The host vectors above die at return: wait for the copies.
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return register_matrix(ctx, std::move(m), handle);
@@ -718,12 +750,49 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
         LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].data, m->data + m->sec_base[s], sizeof(double) * m->sec_dlen[s],
                                        cudaMemcpyDeviceToHost, ctx->stream));
     }
-  std::vector<int64_t> h_row_p(m->n_rows + 1), h_off(m->nnz);
-  std::vector<int32_t> h_col(m->nnz);
-  LAMB_CUDA(ctx, cudaMemcpyAsync(h_row_p.data(), m->row_p, sizeof(int64_t) * (m->n_rows + 1), cudaMemcpyDeviceToHost, ctx->stream));
-  if (m->nnz) {
-    LAMB_CUDA(ctx, cudaMemcpyAsync(h_col.data(), m->col, sizeof(int32_t) * m->nnz, cudaMemcpyDeviceToHost, ctx->stream));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(h_off.data(), m->off, sizeof(int64_t) * m->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+  // Sector indices (1-based int16 columns, 1-based extents) are built on the
+  // device in one array ordered sector by sector, then copied per sector.
+  const int64_t n_seq = (int64_t)m->n_rows * S;
+  std::vector<int64_t> h_bcnt(std::max<int64_t>(n_seq, 1), 0);
+  int16_t* d_col16 = nullptr;
+  int64_t *d_ext = nullptr, *d_dsz = nullptr, *d_bcnt = nullptr, *d_bpos = nullptr, *d_sbase = nullptr;
+  int32_t *d_rb = nullptr, *d_cb = nullptr;
+  struct Tmp {
+    Ctx* c;
+    std::vector<void**> ps;
+    ~Tmp() { for (void** p : ps) if (*p) { cudaFreeAsync(*p, c->stream); *p = nullptr; } }
+  } tmp{ctx, {(void**)&d_col16, (void**)&d_ext, (void**)&d_dsz, (void**)&d_bcnt, (void**)&d_bpos, (void**)&d_sbase,
+              (void**)&d_rb, (void**)&d_cb}};
+  if (n_seq > 0 && m->nnz > 0) {
+    LAMB_TRY(dalloc(ctx, &d_col16, m->nnz));
+    LAMB_TRY(dalloc(ctx, &d_ext, 2 * m->nnz));
+    LAMB_TRY(dalloc(ctx, &d_dsz, n_seq));
+    LAMB_TRY(dalloc(ctx, &d_bcnt, n_seq));
+    LAMB_TRY(dalloc(ctx, &d_bpos, n_seq));
+    LAMB_TRY(dalloc(ctx, &d_sbase, (int64_t)m->sec_base.size()));
+    LAMB_TRY(dalloc(ctx, &d_rb, m->n_rsub + 1));
+    LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(d_sbase, m->sec_base.data(), sizeof(int64_t) * m->sec_base.size(), cudaMemcpyHostToDevice, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
+    k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+                                                                      m->col, m->row_bs, m->col_bs, d_dsz, d_bcnt);
+    LAMB_LAUNCHED(ctx);
+    LAMB_TRY(exclusive_scan_i64(ctx, d_bcnt, d_bpos, n_seq));
+    k_sector_index<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+                                                                        m->col, m->off, m->row_bs, m->col_bs, d_bpos,
+                                                                        d_sbase, d_col16, d_ext);
+    LAMB_LAUNCHED(ctx);
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h_bcnt.data(), d_bcnt, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
+    int64_t first = 0;
+    for (size_t s = 0; s < (size_t)m->n_rsub * S; ++s) {
+      const int64_t nb = m->sec_nblk[s];
+      if (nb) {
+        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].col_i, d_col16 + first, sizeof(int16_t) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].extents, d_ext + 2 * first, sizeof(int64_t) * 2 * nb, cudaMemcpyDeviceToHost, ctx->stream));
+      }
+      first += nb;
+    }
   }
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (int a = 0; a < m->n_rsub; ++a)
@@ -736,27 +805,12 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
       o.n_cols = m->csub_cnt[b];
       if (o.row_blk_sizes && o.n_rows) memcpy(o.row_blk_sizes, &m->h_row_bs[m->rsub_base[a]], o.n_rows);
       if (o.col_blk_sizes && o.n_cols) memcpy(o.col_blk_sizes, &m->h_col_bs[m->csub_base[b]], o.n_cols);
-      const int32_t c0 = m->csub_base[b], c1 = m->csub_base[b + 1];
-      int64_t q = 0;
+      // run lengths of sector (a,b): h_bcnt[rsub_base[a]*S + b*cnt_a + l]
+      const int64_t cnt = m->rsub_cnt[a];
+      const int64_t base = (int64_t)m->rsub_base[a] * S + b * cnt;
       o.row_p[0] = 0;
-      for (int l = 0; l < m->rsub_cnt[a]; ++l) {
-        const int r = m->rsub_base[a] + l;
-        const int bi = m->h_row_bs[r];
-        const int32_t* cb = h_col.data() + h_row_p[r];
-        const int32_t* ce = h_col.data() + h_row_p[r + 1];
-        const int32_t* lo = std::lower_bound(cb, ce, c0);
-        const int32_t* hi = std::lower_bound(lo, ce, c1);
-        for (const int32_t* it = lo; it != hi; ++it) {
-          const int64_t g = h_row_p[r] + (it - cb);
-          const int64_t sz = (int64_t)bi * m->h_col_bs[*it];
-          o.col_i[q] = (int16_t)(*it - c0 + 1);
-          o.extents[2 * q] = h_off[g] - m->sec_base[s] + 1;
-          o.extents[2 * q + 1] = h_off[g] - m->sec_base[s] + sz;
-          ++q;
-        }
-        o.row_p[l + 1] = q;
-      }
-      o.n_blks = q;
+      for (int64_t l = 0; l < cnt; ++l) o.row_p[l + 1] = o.row_p[l] + (m->nnz ? h_bcnt[base + l] : 0);
+      o.n_blks = m->sec_nblk[s];
       o.data_len = m->sec_dlen[s];
     }
   return LAMB_GPU_OK;

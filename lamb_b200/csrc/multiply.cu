@@ -48,7 +48,8 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_count(
     const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
     const double* __restrict__ b_nrm, const int8_t* __restrict__ row_bs, const int8_t* __restrict__ k_bs,
     const int8_t* __restrict__ col_bs, double eps, int filt, int32_t n_words, int64_t* __restrict__ c_cnt,
-    int64_t* __restrict__ s_cnt, int64_t* __restrict__ p_cnt, double* __restrict__ row_flops) {
+    int64_t* __restrict__ s_cnt, int64_t* __restrict__ p_cnt, double* __restrict__ row_flops,
+    unsigned* __restrict__ max_a_len) {
   extern __shared__ uint32_t bm[];
   typedef cub::BlockReduce<int64_t, kSymThreads> RI;
   typedef cub::BlockReduce<double, kSymThreads> RD;
@@ -90,6 +91,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_count(
       s_cnt[i] = tot_kept;
       p_cnt[i] = tot_pairs;
       row_flops[i] = tot_fl;
+      atomicMax(max_a_len, (unsigned)(a_row_p[i + 1] - a_row_p[i]));
     }
     __syncthreads();
   }
@@ -122,28 +124,48 @@ __device__ __forceinline__ int bm_rank(const uint32_t* bm, const int* wpre, int 
   return wpre[j >> 5] + __popc(bm[j >> 5] & ((1u << (j & 31)) - 1u));
 }
 
+// Stack fill, one CTA per C row.  The row's A blocks (column norm, operand
+// word, B-row bounds) are staged in shared memory first, so the pair loops
+// carry one dependent load (the B block) instead of three.  Entries are
+// written one A block at a time (barrier between A blocks), so every C
+// block's stack lists its products in ascending k and consecutive slots of a
+// stack are written close together in time; thread t prefetches its B block
+// of the next A block before the barrier.
+// Shared memory: bitmap and word ranks (n_words each), stack cursors
+// (max_c + 1) and the staged A row (na_max x 32 bytes).
 template <bool IDS>
 __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
     const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
-    const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, const int64_t* __restrict__ c_row_p,
-    const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col, int64_t* __restrict__ stack_p,
-    const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off, Ent* __restrict__ ent,
-    int2* __restrict__ ids) {
-  extern __shared__ uint32_t sm[];
-  uint32_t* bm = sm;
-  int* wpre = (int*)(sm + n_words);
+    const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, int32_t na_max, int32_t nc_max,
+    const int64_t* __restrict__ c_row_p, const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col,
+    int64_t* __restrict__ stack_p, const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off,
+    Ent* __restrict__ ent, int2* __restrict__ ids) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s_anrm = reinterpret_cast<double*>(smem_raw);
+  long long* s_aoff = reinterpret_cast<long long*>(s_anrm + na_max);
+  int64_t* s_bbeg = reinterpret_cast<int64_t*>(s_aoff + na_max);
+  int64_t* s_bend = s_bbeg + na_max;
+  uint32_t* bm = reinterpret_cast<uint32_t*>(s_bend + na_max);
+  int* wpre = reinterpret_cast<int*>(bm + n_words);
   int* cur = wpre + n_words;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kSymThreads / 32;
   for (int64_t i = blockIdx.x; i < n_rows; i += gridDim.x) {
+    const int64_t a0 = a_row_p[i];
+    const int na = (int)(a_row_p[i + 1] - a0);
+    for (int t = tid; t < na; t += kSymThreads) {
+      const int k = a_col[a0 + t];
+      s_anrm[t] = a_nrm[a0 + t];
+      s_aoff[t] = IDS ? 0 : a_offk[a0 + t];
+      s_bbeg[t] = b_row_p[k];
+      s_bend[t] = b_row_p[k + 1];
+    }
     for (int w = tid; w < n_words; w += kSymThreads) bm[w] = 0u;
     __syncthreads();
-    const int64_t a0 = a_row_p[i], a1 = a_row_p[i + 1];
-    for (int64_t ab = a0 + warp; ab < a1; ab += nw) {
-      const int k = a_col[ab];
-      const double na = a_nrm[ab];
-      for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
-        if (keep_pair(na, b_nrm[bb], eps, filt)) {
+    for (int a = warp; a < na; a += nw) {
+      const double x = s_anrm[a];
+      for (int64_t bb = s_bbeg[a] + lane; bb < s_bend[a]; bb += 32)
+        if (keep_pair(x, b_nrm[bb], eps, filt)) {
           const int j = b_col[bb];
           atomicOr(&bm[j >> 5], 1u << (j & 31));
         }
@@ -166,11 +188,10 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     }
     for (int t = tid; t < nc; t += kSymThreads) cur[t] = 0;
     __syncthreads();
-    for (int64_t ab = a0 + warp; ab < a1; ab += nw) {
-      const int k = a_col[ab];
-      const double na = a_nrm[ab];
-      for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
-        if (keep_pair(na, b_nrm[bb], eps, filt)) atomicAdd(&cur[bm_rank(bm, wpre, b_col[bb])], 1);
+    for (int a = warp; a < na; a += nw) {
+      const double x = s_anrm[a];
+      for (int64_t bb = s_bbeg[a] + lane; bb < s_bend[a]; bb += 32)
+        if (keep_pair(x, b_nrm[bb], eps, filt)) atomicAdd(&cur[bm_rank(bm, wpre, b_col[bb])], 1);
     }
     __syncthreads();
     block_excl_scan_smem(cur, nc);
@@ -179,23 +200,44 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     __syncthreads();
     // Entries in k order: one A block at a time; the B row's columns are
     // distinct, so each C position advances at most once per A block.
-    for (int64_t ab = a0; ab < a1; ++ab) {
-      const int k = a_col[ab];
-      const double na = a_nrm[ab];
-      const long long ak = IDS ? 0 : a_offk[ab];
-      for (int64_t bb = b_row_p[k] + tid; bb < b_row_p[k + 1]; bb += kSymThreads)
-        if (keep_pair(na, b_nrm[bb], eps, filt)) {
-          const int p = bm_rank(bm, wpre, b_col[bb]);
+    // Thread t owns B entries t, t + 256, ... of every B row; its first one
+    // of the next A block is loaded before the barrier.
+    int64_t bb = na > 0 ? s_bbeg[0] + tid : 0;
+    bool have = na > 0 && bb < s_bend[0];
+    double nb = have ? b_nrm[bb] : 0.0;
+    int jb = have ? b_col[bb] : 0;
+    for (int a = 0; a < na; ++a) {
+      const double x = s_anrm[a];
+      const long long ak = s_aoff[a];
+      const int64_t bend = s_bend[a];
+      // prefetch of the next A block's first entry for this thread
+      const int64_t nbb = a + 1 < na ? s_bbeg[a + 1] + tid : 0;
+      const bool nhave = a + 1 < na && nbb < s_bend[a + 1];
+      const double nnb = nhave ? b_nrm[nbb] : 0.0;
+      const int njb = nhave ? b_col[nbb] : 0;
+      while (have) {
+        if (keep_pair(x, nb, eps, filt)) {
+          const int p = bm_rank(bm, wpre, jb);
           const int slot = cur[p];
           cur[p] = slot + 1;
           if (IDS)
-            ids[sb + slot] = make_int2((int)ab, (int)bb);
+            ids[sb + slot] = make_int2((int)(a0 + a), (int)bb);
           else
             ent[sb + slot] = Ent{ak, (long long)b_off[bb]};
         }
+        bb += kSymThreads;
+        have = bb < bend;
+        if (have) { nb = b_nrm[bb]; jb = b_col[bb]; }
+      }
       __syncthreads();
+      bb = nbb; have = nhave; nb = nnb; jb = njb;
     }
   }
+}
+
+// Shared memory of k_sym_fill for the given sizes.
+static size_t sym_fill_smem(int32_t n_words, int64_t na_max, int64_t nc_max) {
+  return (size_t)(32 * na_max + 8 * (int64_t)n_words + 4 * (nc_max + 1));
 }
 
 int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, bool filt, bool want_ids,
@@ -232,6 +274,9 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_TRY(dalloc(ctx, &s_cnt, std::max(n_rows, 1)));
   LAMB_TRY(dalloc(ctx, &p_cnt, std::max(n_rows, 1)));
   LAMB_TRY(dalloc(ctx, &rfl, std::max(n_rows, 1)));
+  unsigned* d_max_na = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_max_na, 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(d_max_na, 0, sizeof(unsigned), ctx->stream));
   const int fl = filt ? 1 : 0;
   const size_t smem_count = sizeof(uint32_t) * (size_t)std::max(n_words, 1);
   if (smem_count > 200 * 1024)
@@ -242,9 +287,10 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
       LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count));
     k_sym_count<<<grid, kSymThreads, smem_count, ctx->stream>>>(
         n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, C->row_bs, B->row_bs, C->col_bs, eps, fl,
-        n_words, c_cnt, s_cnt, p_cnt, rfl);
+        n_words, c_cnt, s_cnt, p_cnt, rfl, d_max_na);
     LAMB_LAUNCHED(ctx);
   }
+  unsigned max_na = 0;
   std::vector<int64_t> h_s(n_rows), h_p(n_rows);
   std::vector<double> h_f(n_rows);
   out->h_row_len.assign(n_rows, 0);
@@ -253,6 +299,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_s.data(), s_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_p.data(), p_cnt, sizeof(int64_t) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(h_f.data(), rfl, sizeof(double) * n_rows, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(&max_na, d_max_na, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   trace_mark(ctx, "symbolic count");
@@ -285,16 +332,17 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     LAMB_TRY(dalloc(ctx, &out->ent, std::max<int64_t>(out->n_ent, 1)));
   LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
   trace_mark(ctx, "symbolic allocations");
-  const size_t smem_fill = sizeof(uint32_t) * (size_t)std::max(n_words, 1) * 2 + sizeof(int) * (size_t)(max_c + 1);
+  const size_t smem_fill = sym_fill_smem(std::max(n_words, 1), std::max<int64_t>(max_na, 1), max_c);
   if (smem_fill > 220 * 1024)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
   if (n_rows > 0 && C->nnz > 0) {
     auto kern = want_ids ? k_sym_fill<true> : k_sym_fill<false>;
     if (smem_fill > 48 * 1024)
       LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
-    kern<<<grid, kSymThreads, smem_fill, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms,
-                                                        eps, fl, n_words, C->row_p, s_row_base, C->col, out->stack_p,
-                                                        a_offk, b_meta ? b_meta : B->off, out->ent, out->ids);
+    kern<<<grid, kSymThreads, smem_fill, ctx->stream>>>(
+        n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, eps, fl, n_words, (int32_t)max_na,
+        (int32_t)max_c, C->row_p, s_row_base, C->col, out->stack_p, a_offk, b_meta ? b_meta : B->off, out->ent,
+        out->ids);
     LAMB_LAUNCHED(ctx);
   }
   trace_mark(ctx, "symbolic fill");
@@ -313,6 +361,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     C->data_cap = need;
   }
   dfree(ctx, c_cnt); dfree(ctx, s_cnt); dfree(ctx, p_cnt); dfree(ctx, rfl); dfree(ctx, s_row_base);
+  dfree(ctx, d_max_na);
   trace_mark(ctx, "C data allocation");
   return LAMB_GPU_OK;
 }
@@ -505,7 +554,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
       LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, mp));
     else
       LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false,
-                              max_block(A->h_col_bs)));
+                           max_block(A->h_col_bs)));
     trace_mark(ctx, "numeric");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps, &dropped));
