@@ -70,48 +70,59 @@ def algorithmic_bytes(a, b, c) -> int:
 
 
 class Clocks:
-    """nvidia-smi sampler (200 ms) over the timed region."""
+    """SM clock and throttle-reason sampler (NVML, in-process thread, 200 ms).
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    Started before the warm-up so that NVML is initialised before the timed
+    region; mark() / stop() bracket the timed region and only samples taken
+    inside it are reported."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, device):
-        self.device = device
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        import threading
+        self.rows, self.t0, self.t1 = [], None, None
+        self._stop = threading.Event()
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self._nv, self._h = pynvml, h
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.p = None
+            self._nv = None
+            return
+        self._th = threading.Thread(target=self._run, daemon=True)
+        self._th.start()
+
+    def _run(self):
+        nv, h = self._nv, self._h
+        while not self._stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.rows.append((time.perf_counter(), mhz, rs))
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def mark(self):
+        self.t0 = time.perf_counter()
 
     def stop(self):
-        if self.p is None:
+        self.t1 = time.perf_counter()
+        if self._nv is None:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.flush()
-        rows = []
-        with open(self.f.name) as fh:
-            for line in fh:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
-                except ValueError:
-                    continue
-        os.unlink(self.f.name)
+        self._stop.set()
+        self._th.join(timeout=2)
+        rows = [r for r in self.rows if self.t0 is not None and self.t0 <= r[0] <= self.t1]
+        if not rows:  # timed region shorter than one period: nearest sample after it
+            rows = [r for r in self.rows if r[0] >= (self.t0 or 0)][:1]
         if not rows:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({k for _, _, rs in rows for k, bit in self.REASONS.items() if rs & bit})
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(rows), "source": "NVML"}
 
 
 def measured_peaks():
@@ -252,6 +263,7 @@ def run_ours(args):
         da.set_positions(g.sector_positions(), g.box)
     dc = ctx.create_like(da)
     ext = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local))
+    clk = Clocks(local)
     for _ in range(args.warmup):
         st = ctx.multiply(da, db, dc, wl.eps)
 
@@ -261,7 +273,7 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clk = Clocks(local)
+    clk.mark()
     with torch.cuda.stream(ext):
         e0.record()
     stats = []
@@ -402,10 +414,11 @@ def run_batch(args):
     t0 = time.perf_counter()
     batch = ctx.batch([d[0] for d in devs], [d[1] for d in devs], [d[2] for d in devs], eps=1e-10)
     t_create = time.perf_counter() - t0
+    clk = Clocks(0)
     for _ in range(args.warmup):
         st = batch.execute()
     torch.cuda.synchronize()
-    clk = Clocks(0)
+    clk.mark()
     ms = []
     for _ in range(args.steps):
         ms.append(batch.execute()["ms_total"])

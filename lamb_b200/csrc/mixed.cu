@@ -36,6 +36,9 @@ namespace lamb {
 
 constexpr int kMixWarps = 4;
 constexpr int kMaxSlices = 8;
+// Largest inner length (bytes of a padded plane row) for which the level
+// accumulators of 7 slices stay exact: 7 products of |digit| <= 64 per index.
+constexpr int64_t kLevelInnerMax7 = (int64_t)INT_MAX / (7 * 64 * 64);
 
 __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
@@ -239,26 +242,26 @@ __device__ __forceinline__ void mixed_tile(const int* __restrict__ pa0, const in
   }
 }
 
-// Digit pairs p in [P0, P1) of one 16 x 8 tile with all their accumulators
-// in registers: per window the B digit planes q < S - P0 are loaded once, each
-// A digit plane once, and every (p, q) pair with p + q <= S - 1 runs one mma.
-template <int S, int P0, int P1, bool SWAP>
-__device__ __forceinline__ void mixed_group(const int* __restrict__ pa0, const int* __restrict__ pb0,
-                                            int64_t a_plane_w, int64_t b_plane_w, const Ent* __restrict__ ent,
-                                            int64_t s0, int n, int cap, WordRef* __restrict__ tbl, int TM, int TN,
-                                            int r0, int c0, double (&out)[4]) {
-  constexpr int NQ = S - P0;  // B planes used by the group
+// One 16 x 8 tile for S digits with one int32 accumulator per weight level
+// d = p + q (every pair of a level has the weight 2^(-12-7d)).  A level sums
+// at most S products of |digit| <= 64 per inner index, so it stays exact while
+// the tile's inner length is at most (2^31 - 1) / (S * 4096) (74,898 for
+// S = 7); callers check that bound.  Per window of 8 words every plane of
+// both operands is loaded once and all S(S+1)/2 pairs run.
+template <int S, bool SWAP>
+__device__ __forceinline__ void mixed_tile_levels(const int* __restrict__ pa0, const int* __restrict__ pb0,
+                                                  int64_t a_plane_w, int64_t b_plane_w, const Ent* __restrict__ ent,
+                                                  int64_t s0, int n, int cap, WordRef* __restrict__ tbl, int TM,
+                                                  int TN, int r0, int c0, double (&out)[4]) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   const int ra = r0 + g, rb = r0 + g + 8, cc = c0 + g;
   const bool ok_a = ra < TM, ok_b = rb < TM, ok_c = cc < TN;
-  int acc[P1 - P0][NQ][4];
+  int acc[S][4];
 #pragma unroll
-  for (int p = 0; p < P1 - P0; ++p)
+  for (int d = 0; d < S; ++d)
 #pragma unroll
-    for (int q = 0; q < NQ; ++q)
-#pragma unroll
-      for (int h = 0; h < 4; ++h) acc[p][q][h] = 0;
+    for (int h = 0; h < 4; ++h) acc[d][h] = 0;
   for (int base = 0; base < n; base += cap) {
     const int m = min(cap, n - base);
     const int W = build_words(pa0, pb0, ent, s0 + base, m, tbl, lane);
@@ -269,52 +272,35 @@ __device__ __forceinline__ void mixed_group(const int* __restrict__ pa0, const i
       const int sa = (int)(ta.pbk >> 56), sbw = (int)(tb.pbk >> 56);
       const int* pba = reinterpret_cast<const int*>(ta.pbk & kOffMask);
       const int* pbb = reinterpret_cast<const int*>(tb.pbk & kOffMask);
-      // tile op2 digit planes (B columns; A rows when SWAP)
-      int bq[NQ][2];
+      int a[S][4], bq[S][2];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        const int* o2a = SWAP ? ta.pa + (int64_t)q * a_plane_w : pba + (int64_t)q * b_plane_w;
-        const int* o2b = SWAP ? tb.pa + (int64_t)q * a_plane_w : pbb + (int64_t)q * b_plane_w;
-        bq[q][0] = (va && ok_c) ? __ldg(o2a + (int64_t)cc * sa) : 0;
-        bq[q][1] = (vb && ok_c) ? __ldg(o2b + (int64_t)cc * sbw) : 0;
-      }
-#pragma unroll
-      for (int p = P0; p < P1; ++p) {
+      for (int p = 0; p < S; ++p) {
+        // tile op1 (A rows; B columns when SWAP) and tile op2, digit plane p
         const int* o1a = SWAP ? pba + (int64_t)p * b_plane_w : ta.pa + (int64_t)p * a_plane_w;
         const int* o1b = SWAP ? pbb + (int64_t)p * b_plane_w : tb.pa + (int64_t)p * a_plane_w;
-        int a[4];
-        a[0] = (va && ok_a) ? __ldg(o1a + (int64_t)ra * sa) : 0;
-        a[1] = (va && ok_b) ? __ldg(o1a + (int64_t)rb * sa) : 0;
-        a[2] = (vb && ok_a) ? __ldg(o1b + (int64_t)ra * sbw) : 0;
-        a[3] = (vb && ok_b) ? __ldg(o1b + (int64_t)rb * sbw) : 0;
-#pragma unroll
-        for (int q = 0; q < S - p; ++q) imma16832(acc[p - P0][q], a, bq[q]);
+        const int* o2a = SWAP ? ta.pa + (int64_t)p * a_plane_w : pba + (int64_t)p * b_plane_w;
+        const int* o2b = SWAP ? tb.pa + (int64_t)p * a_plane_w : pbb + (int64_t)p * b_plane_w;
+        a[p][0] = (va && ok_a) ? __ldg(o1a + (int64_t)ra * sa) : 0;
+        a[p][1] = (va && ok_b) ? __ldg(o1a + (int64_t)rb * sa) : 0;
+        a[p][2] = (vb && ok_a) ? __ldg(o1b + (int64_t)ra * sbw) : 0;
+        a[p][3] = (vb && ok_b) ? __ldg(o1b + (int64_t)rb * sbw) : 0;
+        bq[p][0] = (va && ok_c) ? __ldg(o2a + (int64_t)cc * sa) : 0;
+        bq[p][1] = (vb && ok_c) ? __ldg(o2b + (int64_t)cc * sbw) : 0;
       }
+#pragma unroll
+      for (int p = 0; p < S; ++p)
+#pragma unroll
+        for (int q = 0; q < S - p; ++q) imma16832(acc[p + q], a[p], bq[q]);
     }
     __syncwarp();
   }
 #pragma unroll
-  for (int p = P0; p < P1; ++p)
+  for (int h = 0; h < 4; ++h) {
+    double v = 0.0;
 #pragma unroll
-    for (int q = 0; q < S - p; ++q) {
-      const int sh = -12 - 7 * (p + q);
-#pragma unroll
-      for (int h = 0; h < 4; ++h) out[h] += ldexp((double)acc[p - P0][q][h], sh);
-    }
-}
-
-// One 16 x 8 tile for S digits: two pair groups (p < 3 and p >= 3).
-template <int S, bool SWAP>
-__device__ __forceinline__ void mixed_tile_s(const int* __restrict__ pa0, const int* __restrict__ pb0,
-                                             int64_t a_plane_w, int64_t b_plane_w, const Ent* __restrict__ ent,
-                                             int64_t s0, int n, int cap, WordRef* __restrict__ tbl, int TM, int TN,
-                                             int r0, int c0, double (&o)[4]) {
-  constexpr int P1 = S < 3 ? S : 3;
-#pragma unroll
-  for (int h = 0; h < 4; ++h) o[h] = 0.0;
-  mixed_group<S, 0, P1, SWAP>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
-  if (S > 3) mixed_group<S, (S > 3 ? 3 : S - 1), S, SWAP>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM,
-                                                            TN, r0, c0, o);
+    for (int d = S - 1; d >= 0; --d) v += ldexp((double)acc[d][h], -12 - 7 * d);
+    out[h] = v;
+  }
 }
 
 __global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
@@ -323,7 +309,7 @@ __global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
     const int* __restrict__ pa0, const int* __restrict__ pb0, int64_t a_plane_w, int64_t b_plane_w, int s,
     const int64_t* __restrict__ rbase, const int64_t* __restrict__ cbase, const int* __restrict__ ea,
     const int* __restrict__ eb, double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_words,
-    unsigned long long* __restrict__ head) {
+    int kmax4, unsigned long long* __restrict__ head) {
   extern __shared__ WordRef wtbl[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -347,21 +333,16 @@ __global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
     for (int r0 = 0; r0 < TM; r0 += 16)
       for (int c0 = 0; c0 < TN; c0 += 8) {
         double o[4];
-#define LAMB_MIX_CASE(SV)                                                                                       \
-  case SV:                                                                                                      \
-    if (swap) mixed_tile_s<SV, true>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);  \
-    else mixed_tile_s<SV, false>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);      \
-    break;
-        switch (s) {
-          LAMB_MIX_CASE(6)
-          LAMB_MIX_CASE(7)
-          default:
-            if (swap)
-              mixed_tile<true>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
-            else
-              mixed_tile<false>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+        if (s == 7 && (int64_t)n * kmax4 <= kLevelInnerMax7) {
+          if (swap)
+            mixed_tile_levels<7, true>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+          else
+            mixed_tile_levels<7, false>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+        } else if (swap) {
+          mixed_tile<true>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+        } else {
+          mixed_tile<false>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
         }
-#undef LAMB_MIX_CASE
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
           const int tr = r0 + g + 8 * (h >> 1), tc = c0 + 2 * t + (h & 1);
@@ -500,7 +481,7 @@ int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const 
   k_mixed<<<grid, kMixWarps * 32, smem, ctx->stream>>>(
       sym.c_nnz, work, work_c, sym.c_row, C->col, sym.ent, reinterpret_cast<const int*>(mp.a_planes),
       reinterpret_cast<const int*>(mp.b_planes), mp.a_plane / 4, mp.b_plane / 4, mp.s, mp.rbase, mp.cbase, mp.ea,
-      mp.eb, C->data, c_nrm, cap, tbl_words, head);
+      mp.eb, C->data, c_nrm, cap, tbl_words, 4 * wpe, head);
   LAMB_LAUNCHED(ctx);
   dfree(ctx, head);
   return LAMB_GPU_OK;

@@ -130,7 +130,9 @@ __device__ __forceinline__ int bm_rank(const uint32_t* bm, const int* wpre, int 
 // written one A block at a time (barrier between A blocks), so every C
 // block's stack lists its products in ascending k and consecutive slots of a
 // stack are written close together in time; thread t prefetches its B block
-// of the next A block before the barrier.
+// (norm, column, data offset) of the next A block before the barrier.  The
+// stack is written with evict-first stores: it streams through L2 once and
+// would otherwise push out the B index the next rows read.
 // Shared memory: bitmap and word ranks (n_words each), stack cursors
 // (max_c + 1) and the staged A row (na_max x 32 bytes).
 template <bool IDS>
@@ -206,6 +208,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     bool have = na > 0 && bb < s_bend[0];
     double nb = have ? b_nrm[bb] : 0.0;
     int jb = have ? b_col[bb] : 0;
+    long long ob = (!IDS && have) ? b_off[bb] : 0;
     for (int a = 0; a < na; ++a) {
       const double x = s_anrm[a];
       const long long ak = s_aoff[a];
@@ -215,6 +218,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
       const bool nhave = a + 1 < na && nbb < s_bend[a + 1];
       const double nnb = nhave ? b_nrm[nbb] : 0.0;
       const int njb = nhave ? b_col[nbb] : 0;
+      const long long nob = (!IDS && nhave) ? b_off[nbb] : 0;
       while (have) {
         if (keep_pair(x, nb, eps, filt)) {
           const int p = bm_rank(bm, wpre, jb);
@@ -223,14 +227,14 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
           if (IDS)
             ids[sb + slot] = make_int2((int)(a0 + a), (int)bb);
           else
-            ent[sb + slot] = Ent{ak, (long long)b_off[bb]};
+            __stcs(reinterpret_cast<longlong2*>(ent + sb + slot), make_longlong2(ak, ob));
         }
         bb += kSymThreads;
         have = bb < bend;
-        if (have) { nb = b_nrm[bb]; jb = b_col[bb]; }
+        if (have) { nb = b_nrm[bb]; jb = b_col[bb]; if (!IDS) ob = b_off[bb]; }
       }
       __syncthreads();
-      bb = nbb; have = nhave; nb = nnb; jb = njb;
+      bb = nbb; have = nhave; nb = nnb; jb = njb; ob = nob;
     }
   }
 }
