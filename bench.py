@@ -339,7 +339,8 @@ def run_ours(args):
         if not args.no_positions:
             xa.set_positions(pos, g.box)
         xc = ctx.create_like(xa)
-        st_e = ctx.multiply(xa, xb, xc, wl.eps)
+        # async: the download below copies C row chunk by row chunk as the numeric phase completes them
+        st_e = ctx.multiply(xa, xb, xc, wl.eps, gpu.ASYNC)
         c_out = xc.download(out=c_out)
         xc.destroy(); xb.destroy(); xa.destroy()
         if it > 0:

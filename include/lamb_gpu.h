@@ -82,7 +82,7 @@ extern "C" {
 #define LAMB_GPU_MIXED 1u             /* int8 split-slice products, FP64 recombination */
 #define LAMB_GPU_NO_PRODUCT_FILTER 2u /* keep products with |A_ik||B_kj| < eps */
 #define LAMB_GPU_NO_RESULT_FILTER 4u  /* keep C blocks with |C_ij| < eps      */
-#define LAMB_GPU_ASYNC 8u             /* return without synchronising         */
+#define LAMB_GPU_ASYNC 8u             /* return once the work is queued (see lamb_gpu_multiply) */
 #define LAMB_GPU_ACCUMULATE 16u       /* C := C + A.B on C's existing blocks (pattern of C is extended) */
 
 /* One sector of a LAMB matrix in the reference's storage (see above). */
@@ -226,9 +226,15 @@ LAMB_API int32_t lamb_gpu_matrix_load_dbcsr(lamb_gpu_ctx* ctx, const char* path,
                                             int32_t n_x_cubes, lamb_gpu_matrix* handle);
 /* Number of sectors, then per-sector sizes (sizes[n_sectors]). */
 LAMB_API int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, int32_t* n_sectors);
+/* After a LAMB_GPU_ASYNC multiply into `handle` the block counts are those
+ * before the result filter (capacities; data lengths are exact), so the query
+ * does not wait for the multiply. */
 LAMB_API int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_sizes* sizes,
                               int32_t n_sectors);
-/* Fills caller-allocated sectors (out[n_sectors], order as from query). */
+/* Fills caller-allocated sectors (out[n_sectors], order as from query);
+ * out[s].n_blks and data_len return what was written.  A multiply's result is
+ * copied in row chunks, each as soon as the numeric phase has finished it, so
+ * after a LAMB_GPU_ASYNC multiply the transfer overlaps the computation. */
 LAMB_API int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_out* out,
                                  int32_t n_sectors);
 
@@ -239,7 +245,11 @@ LAMB_API int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* ctx, lamb_gpu_matrix han
  * |A_ik|_F*|B_kj|_F < eps and a C block is dropped when |C_ij|_F < eps
  * (both switchable by flags; eps <= 0 disables both).  `c` must be a handle
  * from lamb_gpu_matrix_create_like or a previous multiply; its contents are
- * replaced.  stats may be NULL. */
+ * replaced.  stats may be NULL.  With LAMB_GPU_ASYNC the call returns after
+ * the symbolic phase, once the numeric phase and the result filter are
+ * queued on the context's stream; the statistics then carry no timings,
+ * n_c_blocks counts blocks before the filter and the next call that uses any
+ * matrix of the context (or lamb_gpu_matrix_download on C) completes it. */
 LAMB_API int32_t lamb_gpu_multiply(lamb_gpu_ctx* ctx, lamb_gpu_matrix a, lamb_gpu_matrix b, lamb_gpu_matrix c,
                           double eps, uint32_t flags, lamb_gpu_mult_stats* stats);
 

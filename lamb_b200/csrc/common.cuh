@@ -50,7 +50,16 @@ struct DevMatrix {
   float box[3] = {0, 0, 0};
   std::vector<int32_t> h_order;  // row processing order, empty until computed
   int32_t* order = nullptr;      // device copy of h_order
+  // Result of a multiply computed in row chunks: the data of chunk p in
+  // sector s is [chunk_rng[2*(p*S_all+s)], chunk_rng[2*(p*S_all+s)+1]) relative
+  // to the sector's base; chunk p is complete when the context's chunk_ev[p]
+  // fires (valid while the context's chunk_m points here).
+  int n_chunks = 0;
+  std::vector<int64_t> chunk_rng;
+  const double* chunk_data = nullptr;  // data buffer the ranges refer to
 };
+
+constexpr int kMaxChunks = 8;
 
 // Roles of the context's grow-only scratch buffers (multiply temporaries).
 enum ScratchSlot : int { kScrEnt = 0, kScrWork, kScrWorkC, kScrPlaneA, kScrPlaneB, kScrSlots };
@@ -65,16 +74,31 @@ struct Ctx {
   int64_t launches = 0;  // kernels of this library launched on the context
   cudaEvent_t ev[8] = {};
   bool trace = false;     // LAMB_GPU_TRACE=1 at creation: phase timings on stderr
+  bool trace_host = false; // LAMB_GPU_TRACE=2: host time between marks, no synchronisation
   double trace_t = 0.0;   // host time of the previous trace mark (ms)
   // Multiply temporaries of several GB (stacks, work items, digit planes) are
   // kept between calls: releasing and re-reserving them fragments the
   // stream-ordered pool, which then maps fresh memory at up to a second a call.
   void* scr[kScrSlots] = {};
   size_t scr_bytes[kScrSlots] = {};
+  // Result filter whose host metadata is still on its way (LAMB_GPU_ASYNC):
+  // per-sector kept block counts land in pend_h (pinned) when pend_ev fires.
+  DevMatrix* pend_m = nullptr;
+  int64_t* pend_h = nullptr;
+  size_t pend_cap = 0;
+  cudaEvent_t pend_ev = nullptr;
+  // Chunked numeric phase of the last multiply (downloads overlap it).
+  DevMatrix* chunk_m = nullptr;
+  cudaEvent_t chunk_ev[kMaxChunks] = {};
+  cudaStream_t copy_stream = nullptr;
 };
 
-// With tracing on, waits for the stream and prints the host time since the
-// previous mark; otherwise does nothing.
+// Completes a pending result filter (waits for its counts and updates the
+// matrix's host metadata).  Every entry point reaches it through get_matrix.
+int32_t settle(Ctx* ctx);
+
+// With tracing on, waits for the stream (not with LAMB_GPU_TRACE=2) and
+// prints the host time since the previous mark; otherwise does nothing.
 void trace_mark(Ctx* ctx, const char* what);
 
 // Error helpers: set the message, return the encoded status.
@@ -119,7 +143,8 @@ void dfree(Ctx* ctx, T*& p) {
   p = nullptr;
 }
 
-DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h);
+DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h);  // settles a pending result filter first
+DevMatrix* find_matrix(Ctx* ctx, lamb_gpu_matrix h); // no settle
 void free_matrix_buffers(Ctx* ctx, DevMatrix* m);
 int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h);
 int32_t ensure_norms(Ctx* ctx, DevMatrix* m);
@@ -134,7 +159,12 @@ void copy_structure(DevMatrix* dst, const DevMatrix* r_src, bool rows_from_rows,
 int32_t upload_block_sizes(Ctx* ctx, DevMatrix* m);
 // Sector-major layout for a pattern already in m (row_p/col set): fills off,
 // sec_base/sec_dlen/sec_nblk, data_len.  row_of (optional, [nnz]) gets each block's row.
-int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of);
+// by_order: inside a sector, rows' blocks follow m's processing order (h_order)
+// instead of the local row order; h_base (optional) gets the data offset of
+// every (row subset, column subset, local rank) run, indexed
+// rsub_base[a]*S + n*rsub_cnt[a] + rank.
+int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of, bool by_order = false,
+                            std::vector<int64_t>* h_base = nullptr);
 // Exclusive scan of int64 (in place allowed), via CUB with stream-ordered scratch.
 int32_t exclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int32_t inclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);

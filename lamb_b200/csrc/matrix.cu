@@ -68,16 +68,34 @@ void release_scratch(Ctx* ctx) {
 
 void trace_mark(Ctx* ctx, const char* what) {
   if (!ctx->trace) return;
-  cudaStreamSynchronize(ctx->stream);
+  if (!ctx->trace_host) cudaStreamSynchronize(ctx->stream);
   const double now =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
   std::fprintf(stderr, "[lamb trace] %-28s %10.2f ms\n", what, ctx->trace_t > 0 ? now - ctx->trace_t : 0.0);
   ctx->trace_t = now;
 }
 
-DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h) {
+int32_t settle(Ctx* ctx) {
+  DevMatrix* m = ctx->pend_m;
+  if (!m) return LAMB_GPU_OK;
+  ctx->pend_m = nullptr;
+  LAMB_CUDA(ctx, cudaEventSynchronize(ctx->pend_ev));
+  const size_t n = (size_t)m->n_rsub * m->n_csub;
+  m->sec_nblk.assign(ctx->pend_h, ctx->pend_h + n);
+  int64_t tot = 0;
+  for (int64_t x : m->sec_nblk) tot += x;
+  m->nnz = tot;
+  return LAMB_GPU_OK;
+}
+
+DevMatrix* find_matrix(Ctx* ctx, lamb_gpu_matrix h) {
   auto it = ctx->mats.find(h);
   return it == ctx->mats.end() ? nullptr : it->second.get();
+}
+
+DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h) {
+  settle(ctx);
+  return find_matrix(ctx, h);
 }
 
 void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
@@ -92,6 +110,9 @@ void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
   dfree(ctx, m->order);
   m->h_order.clear();
   m->norms_valid = false;
+  m->n_chunks = 0;
+  m->chunk_rng.clear();
+  if (ctx->chunk_m == m) ctx->chunk_m = nullptr;
 }
 
 int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h) {
@@ -208,13 +229,13 @@ int32_t ensure_norms(Ctx* ctx, DevMatrix* m) {
 __global__ void k_part_sizes(int32_t n_rows, int32_t n_rsub, int32_t S, const int32_t* __restrict__ rsub_base,
                              const int32_t* __restrict__ csub_base, const int64_t* __restrict__ row_p,
                              const int32_t* __restrict__ col, const int8_t* __restrict__ row_bs,
-                             const int8_t* __restrict__ col_bs, int64_t* __restrict__ dsz,
-                             int64_t* __restrict__ bcnt) {
+                             const int8_t* __restrict__ col_bs, const int32_t* __restrict__ lrank,
+                             int64_t* __restrict__ dsz, int64_t* __restrict__ bcnt) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
     int m = 0;
     while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
     const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
-    const int64_t l = r - rsub_base[m];
+    const int64_t l = lrank ? lrank[r] : r - rsub_base[m];
     const int64_t base = (int64_t)rsub_base[m] * S + l;
     const int bi = row_bs[r];
     int n = 0;
@@ -241,12 +262,13 @@ __global__ void k_part_offsets(int32_t n_rows, int32_t n_rsub, int32_t S, const 
                                const int32_t* __restrict__ csub_base, const int64_t* __restrict__ row_p,
                                const int32_t* __restrict__ col, const int8_t* __restrict__ row_bs,
                                const int8_t* __restrict__ col_bs, const int64_t* __restrict__ dbase,
-                               int64_t* __restrict__ off, int32_t* __restrict__ row_of) {
+                               const int32_t* __restrict__ lrank, int64_t* __restrict__ off,
+                               int32_t* __restrict__ row_of) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
     int m = 0;
     while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
     const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
-    const int64_t l = r - rsub_base[m];
+    const int64_t l = lrank ? lrank[r] : r - rsub_base[m];
     const int64_t base = (int64_t)rsub_base[m] * S + l;
     const int bi = row_bs[r];
     int n = 0;
@@ -292,9 +314,20 @@ __global__ void k_sector_index(int32_t n_rows, int32_t n_rsub, int32_t S, const 
   }
 }
 
-int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of) {
+int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of, bool by_order, std::vector<int64_t>* h_base_out) {
   const int S = m->n_csub;
   const int64_t n_seq = (int64_t)m->n_rows * S;
+  // Rank of every row among the rows of its subset, in the processing order
+  // (h_order), when the rows' data should follow that order.
+  std::vector<int32_t> h_rank;
+  int32_t* d_rank = nullptr;
+  if (by_order && (int64_t)m->h_order.size() == m->n_rows && m->n_rows > 0) {
+    h_rank.resize(m->n_rows);
+    std::vector<int32_t> next(m->n_rsub, 0), sub_of(m->n_rows);
+    for (int a = 0; a < m->n_rsub; ++a)
+      for (int r = m->rsub_base[a]; r < m->rsub_base[a + 1]; ++r) sub_of[r] = a;
+    for (int32_t r : m->h_order) h_rank[r] = next[sub_of[r]]++;
+  }
   m->sec_base.assign((size_t)m->n_rsub * S, 0);
   m->sec_dlen.assign((size_t)m->n_rsub * S, 0);
   m->sec_nblk.assign((size_t)m->n_rsub * S, 0);
@@ -307,15 +340,19 @@ int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of) {
   LAMB_TRY(dalloc(ctx, &dsz, n_seq));
   LAMB_TRY(dalloc(ctx, &bcnt, n_seq));
   LAMB_TRY(dalloc(ctx, &dbase, n_seq));
+  if (!h_rank.empty()) {
+    LAMB_TRY(dalloc(ctx, &d_rank, m->n_rows));
+    LAMB_CUDA(ctx, cudaMemcpyAsync(d_rank, h_rank.data(), sizeof(int32_t) * m->n_rows, cudaMemcpyHostToDevice, ctx->stream));
+  }
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
   k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
-                                                                    m->col, m->row_bs, m->col_bs, dsz, bcnt);
+                                                                    m->col, m->row_bs, m->col_bs, d_rank, dsz, bcnt);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, dsz, dbase, n_seq));
   k_part_offsets<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
-                                                                      m->col, m->row_bs, m->col_bs, dbase, m->off,
-                                                                      row_of);
+                                                                      m->col, m->row_bs, m->col_bs, dbase, d_rank,
+                                                                      m->off, row_of);
   LAMB_LAUNCHED(ctx);
   std::vector<int64_t> h_dsz(n_seq), h_bcnt(n_seq), h_dbase(n_seq);
   LAMB_CUDA(ctx, cudaMemcpyAsync(h_dsz.data(), dsz, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
@@ -334,7 +371,8 @@ int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of) {
       m->sec_nblk[s] = nb;
     }
   m->data_len = h_dbase[n_seq - 1] + h_dsz[n_seq - 1];
-  dfree(ctx, d_rb); dfree(ctx, d_cb); dfree(ctx, dsz); dfree(ctx, bcnt); dfree(ctx, dbase);
+  if (h_base_out) *h_base_out = std::move(h_dbase);
+  dfree(ctx, d_rb); dfree(ctx, d_cb); dfree(ctx, dsz); dfree(ctx, bcnt); dfree(ctx, dbase); dfree(ctx, d_rank);
   return LAMB_GPU_OK;
 }
 
@@ -501,7 +539,12 @@ int32_t lamb_gpu_ctx_create(int32_t device, lamb_gpu_ctx** out) {
     return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
-  if (const char* t = std::getenv("LAMB_GPU_TRACE")) ctx->trace = t[0] == '1';
+  for (auto& ev : ctx->chunk_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+  if (const char* t = std::getenv("LAMB_GPU_TRACE")) {
+    ctx->trace = t[0] == '1' || t[0] == '2';
+    ctx->trace_host = t[0] == '2';
+  }
   // Keep freed stream-ordered memory in the pool between calls.
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -516,11 +559,16 @@ int32_t lamb_gpu_ctx_destroy(lamb_gpu_ctx* c) {
   auto* ctx = reinterpret_cast<Ctx*>(c);
   if (!ctx) return LAMB_GPU_OK;
   cudaSetDevice(ctx->device);
+  settle(ctx);
   for (auto& kv : ctx->mats) free_matrix_buffers(ctx, kv.second.get());
   ctx->mats.clear();
   release_scratch(ctx);
   cudaStreamSynchronize(ctx->stream);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+  for (auto& ev : ctx->chunk_ev) cudaEventDestroy(ev);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->pend_ev) cudaEventDestroy(ctx->pend_ev);
+  if (ctx->pend_h) cudaFreeHost(ctx->pend_h);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return LAMB_GPU_OK;
@@ -670,6 +718,7 @@ int32_t lamb_gpu_matrix_create_like(lamb_gpu_ctx* c, lamb_gpu_matrix like, lamb_
 int32_t lamb_gpu_matrix_destroy(lamb_gpu_ctx* c, lamb_gpu_matrix h) {
   auto* ctx = reinterpret_cast<Ctx*>(c);
   if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  settle(ctx);
   auto it = ctx->mats.find(h);
   if (it == ctx->mats.end()) return fail(ctx, LAMB_LEVEL_WARNING, LAMB_TYPE_WRONG_ARGS, "destroy: invalid handle");
   cudaSetDevice(ctx->device);
@@ -698,7 +747,7 @@ int32_t lamb_gpu_matrix_set_positions(lamb_gpu_ctx* c, lamb_gpu_matrix h, const 
 int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* c, lamb_gpu_matrix h, int32_t* n) {
   auto* ctx = reinterpret_cast<Ctx*>(c);
   if (!ctx || !n) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
-  DevMatrix* m = get_matrix(ctx, h);
+  DevMatrix* m = find_matrix(ctx, h);
   if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "invalid handle");
   *n = m->n_rsub * m->n_csub;
   return LAMB_GPU_OK;
@@ -707,7 +756,9 @@ int32_t lamb_gpu_matrix_n_sectors(lamb_gpu_ctx* c, lamb_gpu_matrix h, int32_t* n
 int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sector_sizes* sizes, int32_t n) {
   auto* ctx = reinterpret_cast<Ctx*>(c);
   if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
-  DevMatrix* m = get_matrix(ctx, h);
+  // No settle(): after a LAMB_GPU_ASYNC multiply the block counts are the
+  // counts before the result filter (capacities that suffice for download).
+  DevMatrix* m = find_matrix(ctx, h);
   if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "invalid handle");
   if (!sizes || n != m->n_rsub * m->n_csub)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "query: sizes array must hold n_sectors entries");
@@ -727,7 +778,9 @@ int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sector_
 int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sector_out* out, int32_t n) {
   auto* ctx = reinterpret_cast<Ctx*>(c);
   if (!ctx) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
-  DevMatrix* m = get_matrix(ctx, h);
+  // The data copies may start before a pending result filter completes (the
+  // filter moves no data); settle() comes after they are queued.
+  DevMatrix* m = find_matrix(ctx, h);
   if (!m) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "invalid handle");
   if (!out || n != m->n_rsub * m->n_csub)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: out array must hold n_sectors entries");
@@ -737,19 +790,47 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
     for (int b = 0; b < S; ++b) {
       auto& o = out[a * S + b];
       const size_t s = (size_t)a * S + b;
-      if (o.n_blks < m->sec_nblk[s] || o.data_len < m->sec_dlen[s])
+      if (o.data_len < m->sec_dlen[s])
         return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: capacity below queried size");
-      if ((m->sec_nblk[s] && (!o.col_i || !o.extents)) || (m->sec_dlen[s] && !o.data) || !o.row_p)
+      if ((m->sec_dlen[s] && !o.data) || !o.row_p)
         return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: NULL output array");
     }
-  // Data first (largest copies), straight into the caller's arrays.
-  for (int a = 0; a < m->n_rsub; ++a)
-    for (int b = 0; b < S; ++b) {
-      const size_t s = (size_t)a * S + b;
+  // Data first (largest copies), straight into the caller's arrays.  A
+  // multiply's result computed in row chunks goes chunk by chunk on the copy
+  // stream, each chunk after its event: the transfer overlaps the chunks still
+  // being computed.
+  const size_t n_sec = (size_t)m->n_rsub * S;
+  bool chunked = ctx->chunk_m == m && m->n_chunks > 0 && m->chunk_data == m->data &&
+                 m->chunk_rng.size() == 2 * (size_t)m->n_chunks * n_sec;
+  for (size_t s = 0; chunked && s < n_sec; ++s)  // the chunks must tile every sector's data
+    for (int p = 0; p < m->n_chunks; ++p) {
+      const int64_t b0 = m->chunk_rng[2 * (p * n_sec + s)], b1 = m->chunk_rng[2 * (p * n_sec + s) + 1];
+      const int64_t prev = p ? m->chunk_rng[2 * ((p - 1) * n_sec + s) + 1] : 0;
+      if (b0 != prev || b1 < b0 || (p == m->n_chunks - 1 && b1 != m->sec_dlen[s])) chunked = false;
+    }
+  if (chunked) {
+    for (int p = 0; p < m->n_chunks; ++p) {
+      LAMB_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->chunk_ev[p], 0));
+      for (size_t s = 0; s < n_sec; ++s) {
+        const int64_t b0 = m->chunk_rng[2 * (p * n_sec + s)], b1 = m->chunk_rng[2 * (p * n_sec + s) + 1];
+        if (b1 > b0)
+          LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].data + b0, m->data + m->sec_base[s] + b0, sizeof(double) * (b1 - b0),
+                                         cudaMemcpyDeviceToHost, ctx->copy_stream));
+      }
+    }
+  } else {
+    for (size_t s = 0; s < n_sec; ++s)
       if (m->sec_dlen[s])
         LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].data, m->data + m->sec_base[s], sizeof(double) * m->sec_dlen[s],
                                        cudaMemcpyDeviceToHost, ctx->stream));
-    }
+  }
+  LAMB_TRY(settle(ctx));
+  for (size_t s = 0; s < n_sec; ++s) {
+    if (out[s].n_blks < m->sec_nblk[s])
+      return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: capacity below queried size");
+    if (m->sec_nblk[s] && (!out[s].col_i || !out[s].extents))
+      return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS, "download: NULL output array");
+  }
   // Sector indices (1-based int16 columns, 1-based extents) are built on the
   // device in one array ordered sector by sector, then copied per sector.
   const int64_t n_seq = (int64_t)m->n_rows * S;
@@ -776,7 +857,8 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
     LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
     LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
     k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
-                                                                      m->col, m->row_bs, m->col_bs, d_dsz, d_bcnt);
+                                                                      m->col, m->row_bs, m->col_bs, nullptr, d_dsz,
+                                                                      d_bcnt);
     LAMB_LAUNCHED(ctx);
     LAMB_TRY(exclusive_scan_i64(ctx, d_bcnt, d_bpos, n_seq));
     k_sector_index<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
@@ -795,6 +877,7 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
     }
   }
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_stream));
   for (int a = 0; a < m->n_rsub; ++a)
     for (int b = 0; b < S; ++b) {
       auto& o = out[a * S + b];

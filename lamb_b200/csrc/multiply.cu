@@ -351,7 +351,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   }
   trace_mark(ctx, "symbolic fill");
   LAMB_TRY(dalloc(ctx, &out->c_row, std::max<int64_t>(C->nnz, 1)));
-  LAMB_TRY(layout_sector_major(ctx, C, out->c_row));
+  LAMB_TRY(layout_sector_major(ctx, C, out->c_row, true, &out->h_base));
   trace_mark(ctx, "sector layout");
   if (C->data_len >= kMask40) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C data too large");
   const int64_t need = std::max<int64_t>(C->data_len, 1);
@@ -409,6 +409,14 @@ __global__ void k_build_work(int32_t n_rows, const int32_t* __restrict__ order, 
   }
 }
 
+__global__ void k_order_lens(int32_t n_rows, const int32_t* __restrict__ order, const int64_t* __restrict__ row_p,
+                             int64_t* __restrict__ lens) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n_rows; w += (int64_t)gridDim.x * blockDim.x) {
+    const int r = order[w];
+    lens[w] = row_p[r + 1] - row_p[r];
+  }
+}
+
 int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
                    int32_t** work_c, bool use_scratch) {
   const int n = C->n_rows;
@@ -422,36 +430,48 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
   if (sym.c_nnz == 0 || n == 0) return LAMB_GPU_OK;
   if ((int)order_src->h_order.size() != n || !order_src->order)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "work list: row order missing");
-  std::vector<int64_t> cum(n + 1, 0);
-  for (int w = 0; w < n; ++w) cum[w + 1] = cum[w] + sym.h_row_len[order_src->h_order[w]];
-  int64_t* d_cum = nullptr;
-  LAMB_TRY(dalloc(ctx, &d_cum, n + 1));
-  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cum, cum.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, ctx->stream));
+  // first work item of every row position: exclusive scan of the C row
+  // lengths taken in the processing order (on the device, no host round trip)
+  int64_t *d_len = nullptr, *d_cum = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_len, n));
+  LAMB_TRY(dalloc(ctx, &d_cum, n));
+  k_order_lens<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, C->row_p, d_len);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, d_len, d_cum, n));
   k_build_work<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, d_cum, C->row_p, C->col, C->off,
                                                             C->row_bs, C->col_bs, sym.stack_p, *work, *work_c);
   LAMB_LAUNCHED(ctx);
-  // cum must outlive the launch: stream-ordered free.
+  dfree(ctx, d_len);
   dfree(ctx, d_cum);
-  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return LAMB_GPU_OK;
 }
 
 // ---- result filter ----------------------------------------------------------------------
-// Keeps C block c iff !(c_nrm[c] < eps).  Counts per (row, column subset)
-// give the new row pointers and per-sector block counts; the data stay where
-// they are (extents may leave holes in a sector's data, as LAMB's data
-// stores allow).
+// Keeps C block c iff !(c_nrm[c] < eps).  Entirely on the device: kept counts
+// per (row, column subset), new row pointers by a scan, the compacted index,
+// and per-sector counts that reach the host asynchronously (settle() applies
+// them).  The data stay where they are (extents may leave holes in a
+// sector's data, as LAMB's data stores allow).
 __global__ void k_keep_counts(int32_t n_rows, int32_t S, const int32_t* __restrict__ csub_base,
+                              const int32_t* __restrict__ rsub_base, int32_t n_rsub,
                               const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
-                              const double* __restrict__ c_nrm, double eps, int64_t* __restrict__ keep_rn) {
+                              const double* __restrict__ c_nrm, double eps, int64_t* __restrict__ row_kept,
+                              unsigned long long* __restrict__ sec_kept) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+    int m = 0;
+    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
     int n = 0;
-    int64_t k = 0;
+    int64_t k = 0, tot = 0;
     for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      while (col[b] >= csub_base[n + 1]) { keep_rn[r * S + n] = k; k = 0; ++n; }
+      while (col[b] >= csub_base[n + 1]) {
+        if (k) atomicAdd(&sec_kept[(int64_t)m * S + n], (unsigned long long)k);
+        tot += k; k = 0; ++n;
+      }
       k += !(c_nrm[b] < eps);
     }
-    for (; n < S; ++n) { keep_rn[r * S + n] = k; k = 0; }
+    if (k) atomicAdd(&sec_kept[(int64_t)m * S + n], (unsigned long long)k);
+    tot += k;
+    row_kept[r + 1] = tot;
   }
 }
 
@@ -466,48 +486,138 @@ __global__ void k_compact(int32_t n_rows, const int64_t* __restrict__ row_p, con
   }
 }
 
-int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps, int64_t* dropped) {
-  *dropped = 0;
+int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps) {
   const int S = C->n_csub;
-  const int64_t n = (int64_t)C->n_rows * S;
-  if (C->nnz == 0 || n == 0) return LAMB_GPU_OK;
-  int64_t* keep_rn = nullptr;
-  int32_t* d_cb = nullptr;
-  LAMB_TRY(dalloc(ctx, &keep_rn, n));
-  LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
-  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, C->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
-  k_keep_counts<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, S, d_cb, C->row_p, C->col, c_nrm, eps, keep_rn);
-  LAMB_LAUNCHED(ctx);
-  std::vector<int64_t> h(n);
-  LAMB_CUDA(ctx, cudaMemcpyAsync(h.data(), keep_rn, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
-  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  std::vector<int64_t> nrp(C->n_rows + 1, 0);
-  std::vector<int64_t> snb((size_t)C->n_rsub * S, 0);
-  int a = 0;
-  for (int r = 0; r < C->n_rows; ++r) {
-    while (a + 1 < C->n_rsub && C->rsub_base[a + 1] <= r) ++a;
-    int64_t k = 0;
-    for (int c = 0; c < S; ++c) { k += h[(int64_t)r * S + c]; snb[(size_t)a * S + c] += h[(int64_t)r * S + c]; }
-    nrp[r + 1] = nrp[r] + k;
+  const size_t n_sec = (size_t)C->n_rsub * S;
+  if (C->nnz == 0 || C->n_rows == 0 || n_sec == 0) return LAMB_GPU_OK;
+  LAMB_TRY(settle(ctx));
+  if (ctx->pend_cap < n_sec) {
+    if (ctx->pend_h) cudaFreeHost(ctx->pend_h);
+    ctx->pend_h = nullptr;
+    ctx->pend_cap = 0;
+    LAMB_CUDA(ctx, cudaMallocHost(&ctx->pend_h, sizeof(int64_t) * n_sec));
+    ctx->pend_cap = n_sec;
   }
-  const int64_t kept = nrp[C->n_rows];
-  *dropped = C->nnz - kept;
-  if (*dropped == 0) { dfree(ctx, keep_rn); dfree(ctx, d_cb); return LAMB_GPU_OK; }
-  int64_t* d_nrp = nullptr;
-  int32_t* ncol = nullptr;
-  int64_t* noff = nullptr;
-  LAMB_TRY(dalloc(ctx, &d_nrp, C->n_rows + 1));
-  LAMB_TRY(dalloc(ctx, &ncol, std::max<int64_t>(kept, 1)));
-  LAMB_TRY(dalloc(ctx, &noff, std::max<int64_t>(kept, 1)));
-  LAMB_CUDA(ctx, cudaMemcpyAsync(d_nrp, nrp.data(), sizeof(int64_t) * (C->n_rows + 1), cudaMemcpyHostToDevice, ctx->stream));
-  k_compact<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, C->off, c_nrm, eps, d_nrp, ncol, noff);
+  if (!ctx->pend_ev) LAMB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->pend_ev, cudaEventDisableTiming));
+  int64_t *row_kept = nullptr, *nrp = nullptr, *noff = nullptr;
+  unsigned long long* sec_kept = nullptr;
+  int32_t *d_cb = nullptr, *d_rb = nullptr, *ncol = nullptr;
+  LAMB_TRY(dalloc(ctx, &row_kept, (int64_t)C->n_rows + 1));
+  LAMB_TRY(dalloc(ctx, &nrp, (int64_t)C->n_rows + 1));
+  LAMB_TRY(dalloc(ctx, &sec_kept, (int64_t)n_sec));
+  LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
+  LAMB_TRY(dalloc(ctx, &d_rb, C->n_rsub + 1));
+  LAMB_TRY(dalloc(ctx, &ncol, C->nnz));
+  LAMB_TRY(dalloc(ctx, &noff, C->nnz));
+  // csub_base / rsub_base are members of C: they outlive the copies.
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, C->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, C->rsub_base.data(), sizeof(int32_t) * (C->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemsetAsync(row_kept, 0, sizeof(int64_t), ctx->stream));
+  LAMB_CUDA(ctx, cudaMemsetAsync(sec_kept, 0, sizeof(unsigned long long) * n_sec, ctx->stream));
+  k_keep_counts<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, S, d_cb, d_rb, C->n_rsub, C->row_p,
+                                                                    C->col, c_nrm, eps, row_kept, sec_kept);
   LAMB_LAUNCHED(ctx);
+  LAMB_TRY(inclusive_scan_i64(ctx, row_kept, nrp, (int64_t)C->n_rows + 1));
+  k_compact<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, C->off, c_nrm, eps, nrp,
+                                                                ncol, noff);
+  LAMB_LAUNCHED(ctx);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(ctx->pend_h, sec_kept, sizeof(int64_t) * n_sec, cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaEventRecord(ctx->pend_ev, ctx->stream));
   dfree(ctx, C->row_p); dfree(ctx, C->col); dfree(ctx, C->off);
-  C->row_p = d_nrp; C->col = ncol; C->off = noff;
-  C->nnz = kept;
-  C->sec_nblk = snb;
+  C->row_p = nrp; C->col = ncol; C->off = noff;
   C->norms_valid = false;
-  dfree(ctx, keep_rn); dfree(ctx, d_cb);
+  dfree(ctx, row_kept); dfree(ctx, sec_kept); dfree(ctx, d_cb); dfree(ctx, d_rb);
+  ctx->pend_m = C;
+  return LAMB_GPU_OK;
+}
+
+// ---- FP64 numeric phase in row chunks --------------------------------------------------
+// The work list (processing order) is cut at row boundaries into up to
+// kMaxChunks launches of about equal C-block count; an event after each marks
+// its rows' C data complete.  Inside a sector, C's data follow the same
+// processing order (layout_sector_major by_order), so chunk p's data in
+// sector s is one contiguous range; downloads copy a chunk as soon as its
+// event fires, overlapping the transfer with the remaining chunks.
+static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym,
+                              const Work* work, const int32_t* work_c, double* c_nrm) {
+  const int mi = max_block(A->h_col_bs);
+  const int n = C->n_rows, S = C->n_csub, R = C->n_rsub;
+  const size_t n_sec = (size_t)R * S;
+  C->n_chunks = 0;
+  C->chunk_rng.clear();
+  const bool layout_ok = (int64_t)C->h_order.size() == n && (int64_t)sym.h_base.size() == (int64_t)n * S && n > 0;
+  const int P = (layout_ok && sym.c_nnz >= 4 * kMaxChunks) ? kMaxChunks : 1;
+  if (P == 1) {
+    LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false, mi));
+    if (layout_ok) {
+      C->n_chunks = 1;
+      C->chunk_rng.assign(2 * n_sec, 0);
+      for (size_t s2 = 0; s2 < n_sec; ++s2) C->chunk_rng[2 * s2 + 1] = C->sec_dlen[s2];
+      LAMB_CUDA(ctx, cudaEventRecord(ctx->chunk_ev[0], ctx->stream));
+      C->chunk_data = C->data;
+      ctx->chunk_m = C;
+    }
+    return LAMB_GPU_OK;
+  }
+  // chunk boundaries in processing positions, by cumulative C blocks
+  std::vector<int> q(P + 1, n);
+  q[0] = 0;
+  {
+    int64_t acc = 0;
+    int p = 1;
+    for (int w = 0; w < n && p < P; ++w) {
+      acc += sym.h_row_len[C->h_order[w]];
+      while (p < P && acc * P >= (int64_t)p * sym.c_nnz) q[p++] = w + 1;
+    }
+  }
+  // rows of each subset before every boundary
+  std::vector<int32_t> sub_of(n);
+  for (int a = 0; a < R; ++a)
+    for (int r = C->rsub_base[a]; r < C->rsub_base[a + 1]; ++r) sub_of[r] = a;
+  std::vector<int64_t> before((size_t)(P + 1) * R, 0);  // rows of subset a at positions < q[p]
+  {
+    std::vector<int64_t> cnt(R, 0);
+    int p = 0;
+    for (int w = 0; w <= n; ++w) {
+      while (p <= P && q[p] == w) {
+        for (int a = 0; a < R; ++a) before[(size_t)p * R + a] = cnt[a];
+        ++p;
+      }
+      if (w < n) ++cnt[sub_of[C->h_order[w]]];
+    }
+  }
+  C->chunk_rng.assign(2 * (size_t)P * n_sec, 0);
+  for (int p = 0; p < P; ++p)
+    for (int a = 0; a < R; ++a)
+      for (int b = 0; b < S; ++b) {
+        const size_t s2 = (size_t)a * S + b;
+        const int64_t cnt_a = C->rsub_cnt[a];
+        auto at = [&](int64_t rank) -> int64_t {  // data offset in the sector before local rank `rank`
+          if (rank >= cnt_a) return C->sec_dlen[s2];
+          return sym.h_base[(size_t)C->rsub_base[a] * S + (size_t)b * cnt_a + rank] - C->sec_base[s2];
+        };
+        C->chunk_rng[2 * ((size_t)p * n_sec + s2)] = at(before[(size_t)p * R + a]);
+        C->chunk_rng[2 * ((size_t)p * n_sec + s2) + 1] = at(before[(size_t)(p + 1) * R + a]);
+      }
+  // C blocks before every boundary (work items are in processing order)
+  std::vector<int64_t> item(P + 1, 0);
+  {
+    int64_t acc = 0;
+    int p = 1;
+    for (int w = 0; w < n; ++w) {
+      acc += sym.h_row_len[C->h_order[w]];
+      while (p < P && q[p] == w + 1) item[p++] = acc;
+    }
+    item[P] = sym.c_nnz;
+  }
+  for (int p = 0; p < P; ++p) {
+    LAMB_TRY(run_stacked(ctx, item[p + 1] - item[p], work + item[p], work_c + item[p], sym.ent, A->data, B->data,
+                         C->data, c_nrm, false, false, mi));
+    LAMB_CUDA(ctx, cudaEventRecord(ctx->chunk_ev[p], ctx->stream));
+  }
+  C->n_chunks = P;
+  C->chunk_data = C->data;
+  ctx->chunk_m = C;
   return LAMB_GPU_OK;
 }
 
@@ -534,6 +644,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   MixedPlanes mp;
   const bool mixed = (flags & LAMB_GPU_MIXED) != 0;
   sym.use_scratch = true;
+  LAMB_TRY(settle(ctx));
   auto body = [&]() -> int32_t {
     trace_mark(ctx, "multiply: start");
     LAMB_TRY(check_compatible(ctx, A, B));
@@ -557,11 +668,10 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
     if (mixed)
       LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, mp));
     else
-      LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false,
-                           max_block(A->h_col_bs)));
+      LAMB_TRY(numeric_chunks(ctx, A, B, C, sym, work, work_c, c_nrm));
     trace_mark(ctx, "numeric");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
-    if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps, &dropped));
+    if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps));
     trace_mark(ctx, "result filter");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
     return LAMB_GPU_OK;
@@ -573,6 +683,13 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   free_symbolic(ctx, sym);
   if (rc != LAMB_GPU_OK) return rc;
   C->norms_valid = false;
+  // Without LAMB_GPU_ASYNC the filter's counts are applied now; with it the
+  // next call that touches a matrix applies them.
+  const int64_t c_before = sym.c_nnz;
+  if (timed) {
+    LAMB_TRY(settle(ctx));
+    dropped = c_before - C->nnz;
+  }
   st.n_products = sym.n_ent;
   st.n_products_skipped = sym.n_pairs - sym.n_ent;
   st.n_c_blocks = C->nnz;

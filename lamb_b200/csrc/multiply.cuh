@@ -38,6 +38,7 @@ struct Symbolic {
   int2* ids = nullptr;         // [n_ent] when ids were requested
   int32_t* c_row = nullptr;    // [c_nnz] row of every C block
   std::vector<int64_t> h_row_len;  // C blocks per row (host)
+  std::vector<int64_t> h_base;     // C data offset of every (row subset, column subset, rank) run
   bool use_scratch = false;    // set before symbolic_phase: ent lives in the context's scratch
 };
 void free_symbolic(Ctx* ctx, Symbolic& s);
@@ -95,8 +96,9 @@ void free_slices(Ctx* ctx, MixedPlanes* mp);
 int32_t pack_plane_meta(Ctx* ctx, const DevMatrix* A, const MixedPlanes& mp, int64_t** a_meta);
 int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,
                       const int32_t* work_c, double* c_nrm, const MixedPlanes& mp);
-// Drops C blocks with c_nrm < eps from the index (data stay in place).
-int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps, int64_t* dropped);
+// Drops C blocks with c_nrm < eps from the index (data stay in place), on the
+// device; C's host block counts are updated by settle() (pending until then).
+int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps);
 // Full multiply on device handles (used by the C ABI, purification and batches).
 int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double eps, uint32_t flags,
                       lamb_gpu_mult_stats* stats);

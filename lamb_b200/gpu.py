@@ -329,6 +329,13 @@ class DeviceMatrix:
             outs.append(o)
         arr = (CSectorOut * len(outs))(*outs)
         self.ctx.check(lib().lamb_gpu_matrix_download(self.ctx.handle, self.h, arr, len(outs)))
+        # after an asynchronous multiply the queried block counts are capacities:
+        # keep what the download wrote
+        for i, s in enumerate(secs):
+            nb = int(arr[i].n_blks)
+            if nb != s.col_i.shape[0]:
+                secs[i] = Sector(s.subset_row, s.subset_col, s.row_blk_sizes, s.col_blk_sizes, s.row_p,
+                                 s.col_i[:nb], s.extents[:nb], s.data)
         return LambMatrix(secs, "C")
 
     def set_positions(self, xyz: np.ndarray, box) -> None:
