@@ -89,3 +89,23 @@ def test_masked_adjoint_matches_dense(gpu_ctx):
     assert [s.n_blks for s in got_a.sectors] == [s.n_blks for s in a.sectors]
     assert np.linalg.norm(got_a.to_dense() - ref_a) / np.linalg.norm(ref_a) < 1e-13
     assert np.linalg.norm(got_b.to_dense() - ref_b) / np.linalg.norm(ref_b) < 1e-13
+
+
+def test_mcweeny_mixed_early_steps_match_fp64(gpu_ctx):
+    """Purification with int8-slice products in the early steps and an FP64
+    tail reaches the all-FP64 density matrix and band energy Tr(P.H)."""
+    g = WaterGeometry(48, None, 5.5, seed=6)
+    h = gapped_hamiltonian(g, 3)
+    dh = gpu_ctx.upload(h)
+    p64, pmx = gpu_ctx.create_like(dh), gpu_ctx.create_like(dh)
+    r64 = gpu_ctx.purify(dh, p64, mu=0.0, steps=30, fp64_tail=30, eps=1e-10)
+    rmx = gpu_ctx.purify(dh, pmx, mu=0.0, steps=30, fp64_tail=5, eps=1e-10)
+    assert rmx["steps_mixed"] == 25 and r64["steps_mixed"] == 0
+    rel = gpu_ctx.diff_frobenius(pmx, p64) / gpu_ctx.frobenius(p64)
+    e64, emx = gpu_ctx.trace_product(p64, dh), gpu_ctx.trace_product(pmx, dh)
+    assert rel < 1e-9
+    assert abs(emx - e64) <= 1e-9 * abs(e64)
+    assert abs(rmx["trace"] - r64["trace"]) < 1e-8
+    assert rmx["idempotency"] < 1e-8
+    for m in (pmx, p64, dh):
+        m.destroy()
