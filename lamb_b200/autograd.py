@@ -262,3 +262,41 @@ class PurifyTrace(torch.autograd.Function):
         for m in [g, pk, dh] + list(cps.values()):
             m.destroy()
         return torch.from_numpy(_flat_on(h_pat, gh)) * gl, None, None
+
+
+def dense_index(m: LambMatrix):
+    """(row, col) in m.to_dense() of every value of m's concatenated sector data
+    (-1 for values outside any block)."""
+    rbs, cbs = m.subset_blk_sizes(0), m.subset_blk_sizes(1)
+    ro = [np.concatenate([[0], np.cumsum(b.astype(np.int64))]) for b in rbs]
+    co = [np.concatenate([[0], np.cumsum(b.astype(np.int64))]) for b in cbs]
+    rb = np.concatenate([[0], np.cumsum([o[-1] for o in ro])])
+    cb = np.concatenate([[0], np.cumsum([o[-1] for o in co])])
+    idx_r, idx_c = [], []
+    for s in m.sectors:
+        r_ = np.full(s.data.shape[0], -1, np.int64)
+        c_ = np.full(s.data.shape[0], -1, np.int64)
+        rows = s.block_rows()
+        for b in range(s.n_blks):
+            r, c = int(rows[b]), int(s.col_i[b]) - 1
+            mm, nn = int(s.row_blk_sizes[r]), int(s.col_blk_sizes[c])
+            f = int(s.extents[b, 0]) - 1
+            pp, qq = np.meshgrid(np.arange(mm), np.arange(nn), indexing="ij")
+            r_[f + qq.ravel() * mm + pp.ravel()] = rb[s.subset_row - 1] + ro[s.subset_row - 1][r] + pp.ravel()
+            c_[f + qq.ravel() * mm + pp.ravel()] = cb[s.subset_col - 1] + co[s.subset_col - 1][c] + qq.ravel()
+        idx_r.append(r_)
+        idx_c.append(c_)
+    return np.concatenate(idx_r), np.concatenate(idx_c)
+
+
+def dense_purify_loss(h_vals: torch.Tensor, ri, ci, n: int, lam: float, steps: int, mu: float = 0.0) -> torch.Tensor:
+    """The same L(H) = Tr(P_K H) with dense torch matrices (FP64 reference gradient)."""
+    dev = h_vals.device
+    eye = torch.eye(n, dtype=torch.float64, device=dev)
+    H = torch.zeros(n, n, dtype=torch.float64, device=dev).index_put(
+        (torch.as_tensor(ri, device=dev), torch.as_tensor(ci, device=dev)), h_vals)
+    P = 0.5 * lam * (mu * eye - H) + 0.5 * eye
+    for _ in range(steps):
+        P2 = P @ P
+        P = 3 * P2 - 2 * P2 @ P
+    return torch.trace(P @ H)

@@ -14,10 +14,15 @@
 // mma.m16n8k32 .s8.s8.s32; the recombination runs in FP64.  Pairs with
 // p + q > s+1 are dropped: their weight is below 2^-(12+7s).
 //
-// Plane layout: A block (M x ke) as M rows of pad4(ke) int8 (row-major), B
-// block (ke x N) as N columns of pad4(ke) int8, so that every 32-bit word is
-// four consecutive inner indices of one row (A) or one column (B) -- the
-// operand words of the m16n8k32 fragments:
+// Plane layout: A block (M x ke) as M rows of pad4(ke) inner indices, B block
+// (ke x N) as N columns of pad4(ke) inner indices; every 32-bit word holds
+// four consecutive inner indices of one row (A) or one column (B) of one
+// digit plane -- the operand words of the m16n8k32 fragments -- and the
+// words of all 8 planes (planes >= s are zero) of one (row, word) position
+// are interleaved in 32 bytes, so one lane fetches every plane of its
+// fragment word with two 16-byte loads:
+//   byte(row ln, inner kc, plane p) = 8*soff + (ln*pad4(ke)/4 + kc/4)*32 + 4p + kc%4
+// (soff: the block's offset in a single plane).  Fragment words:
 //   op1 a0,a1,a2,a3 = words (g, t), (g+8, t), (g, 4+t), (g+8, 4+t)
 //   op2 b0,b1       = words (col g, t), (col g, 4+t)
 //   out c0..c3      = (g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1)
@@ -111,14 +116,14 @@ __global__ void k_plane_sizes(int32_t n_rows, const int64_t* __restrict__ row_p,
     }
 }
 
-// Digits of one block into every plane.  a_side: x(p, kc) = A(p,kc) 2^-ea_p,
-// stored at [p][kc]; else x(c, kc) = B(kc,c) 2^-eb_c, stored at [c][kc].
+// Digits of one block into the interleaved planes.  a_side: line p holds
+// x(p, kc) = A(p,kc) 2^-ea_p; else line c holds x(c, kc) = B(kc,c) 2^-eb_c.
 __global__ void k_digits(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                          const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                          const int8_t* __restrict__ col_bs, const double* __restrict__ d,
                          const int64_t* __restrict__ rbase, const int64_t* __restrict__ cbase,
                          const int* __restrict__ e_row, const int* __restrict__ e_col, int a_side,
-                         const int64_t* __restrict__ soff, int64_t plane_bytes, int s, int8_t* __restrict__ planes) {
+                         const int64_t* __restrict__ soff, int s, int8_t* __restrict__ planes) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
@@ -129,20 +134,31 @@ __global__ void k_digits(int32_t n_rows, const int64_t* __restrict__ row_p, cons
       const int lines = a_side ? rb : cb;  // stored rows
       const int ke = a_side ? cb : rb;     // inner size
       const int kp = pad4(ke);
-      for (int e = lane; e < lines * kp; e += 32) {
-        const int ln = e / kp, kc = e % kp;
-        double v = 0.0;
-        if (kc < ke) {
-          v = a_side ? x[(int64_t)kc * rb + ln] : x[(int64_t)ln * rb + kc];
-          v = ldexp(v, -(a_side ? e_row[rbase[r] + ln] : e_col[cbase[j] + ln]));
+      // one lane per (line, word): 4 inner indices x 8 planes = 32 bytes, two 16-byte stores
+      const int nwl = kp >> 2;
+      for (int e = lane; e < lines * nwl; e += 32) {
+        const int ln = e / nwl, w = e % nwl;
+        const int e_sc = a_side ? e_row[rbase[r] + ln] : e_col[cbase[j] + ln];
+        unsigned word[kMaxSlices];
+#pragma unroll
+        for (int p = 0; p < kMaxSlices; ++p) word[p] = 0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int kc = 4 * w + q;
+          double v = 0.0;
+          if (kc < ke) v = ldexp(a_side ? x[(int64_t)kc * rb + ln] : x[(int64_t)ln * rb + kc], -e_sc);
+          // digits: 2^6 v, then 7 bits per step; every step is exact in FP64
+          double t = ldexp(v, 6);
+#pragma unroll
+          for (int p = 0; p < kMaxSlices; ++p) {
+            const double dg = p < s ? rint(t) : 0.0;
+            word[p] |= (unsigned)(uint8_t)(int8_t)dg << (8 * q);
+            t = ldexp(t - dg, 7);
+          }
         }
-        // digits: 2^6 v, then 7 bits per step; every step is exact in FP64
-        double t = ldexp(v, 6);
-        for (int p = 0; p < s; ++p) {
-          const double dg = rint(t);
-          planes[(int64_t)p * plane_bytes + soff[b] + e] = (int8_t)dg;
-          t = ldexp(t - dg, 7);
-        }
+        int4* dst = reinterpret_cast<int4*>(planes + 8 * soff[b] + ((int64_t)ln * nwl + w) * 32);
+        dst[0] = make_int4((int)word[0], (int)word[1], (int)word[2], (int)word[3]);
+        dst[1] = make_int4((int)word[4], (int)word[5], (int)word[6], (int)word[7]);
       }
     }
   }
@@ -150,8 +166,8 @@ __global__ void k_digits(int32_t n_rows, const int64_t* __restrict__ row_p, cons
 
 // ---- numeric kernel ---------------------------------------------------------------------
 struct WordRef {
-  const int* pa;            // A plane 0 word (row 0, this word)
-  unsigned long long pbk;   // B plane 0 word (col 0, this word) | row stride in words << 56
+  const int4* pa;           // A word group (row 0, this word): 8 plane words, 32 bytes
+  unsigned long long pbk;   // B word group (column 0, this word) | row stride in int4 units << 56
 };
 
 __device__ __forceinline__ void imma16832(int (&c)[4], const int (&a)[4], const int (&b)[2]) {
@@ -161,8 +177,8 @@ __device__ __forceinline__ void imma16832(int (&c)[4], const int (&a)[4], const 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Word table of one chunk: words of every entry's plane-0 blocks, concatenated.
-__device__ __forceinline__ int build_words(const int* __restrict__ pa0, const int* __restrict__ pb0,
+// Word table of one chunk: the word groups of every entry's blocks, concatenated.
+__device__ __forceinline__ int build_words(const int4* __restrict__ pa0, const int4* __restrict__ pb0,
                                            const Ent* __restrict__ ent, int64_t first, int m,
                                            WordRef* __restrict__ tbl, int lane) {
   Ent x{0, 0};
@@ -171,19 +187,57 @@ __device__ __forceinline__ int build_words(const int* __restrict__ pa0, const in
   const int nw = (ke + 3) >> 2;
   const int incl = warp_incl_scan(nw, lane);
   const int W = __shfl_sync(0xffffffffu, incl, 31);
-  const int* pa = pa0 + ((x.a & kOffMask) >> 2);
-  const int* pb = pb0 + (x.b >> 2);
-  const unsigned long long sb = (unsigned long long)nw << 56;
-  for (int w = 0, k = incl - nw; w < nw; ++w, ++k) tbl[k] = WordRef{pa + w, (unsigned long long)(pb + w) | sb};
+  // 8 * soff bytes = soff / 2 int4 (soff is a multiple of 4)
+  const int4* pa = pa0 + ((x.a & kOffMask) >> 1);
+  const int4* pb = pb0 + (x.b >> 1);
+  const unsigned long long sb = (unsigned long long)(2 * nw) << 56;
+  for (int w = 0, k = incl - nw; w < nw; ++w, ++k)
+    tbl[k] = WordRef{pa + 2 * w, (unsigned long long)(pb + 2 * w) | sb};
   __syncwarp();
   return W;
 }
 
-// 16 tile rows (r0..) x 8 tile columns (c0..) of one C block.  SWAP: tile rows
-// are the block's columns (B side), tile columns the block's rows (A side).
+// The 8 plane words of one fragment word (two 16-byte loads), zero when absent.
+__device__ __forceinline__ void ld_group(const int4* p, bool ok, int (&w)[8]) {
+  int4 lo = make_int4(0, 0, 0, 0), hi = make_int4(0, 0, 0, 0);
+  if (ok) {
+    lo = __ldg(p);
+    hi = __ldg(p + 1);
+  }
+  w[0] = lo.x; w[1] = lo.y; w[2] = lo.z; w[3] = lo.w;
+  w[4] = hi.x; w[5] = hi.y; w[6] = hi.z; w[7] = hi.w;
+}
+
+// Fragment words of one 8-word window for every plane: op1 (16 tile rows:
+// A rows, or B columns when SWAP) and op2 (8 tile columns).
 template <bool SWAP>
-__device__ __forceinline__ void mixed_tile(const int* __restrict__ pa0, const int* __restrict__ pb0,
-                                           int64_t a_plane_w, int64_t b_plane_w, int s,
+__device__ __forceinline__ void load_window(const WordRef* __restrict__ tbl, int W, int w0, int t, int ra, int rb,
+                                            int cc, bool ok_a, bool ok_b, bool ok_c, int (&a)[4][8],
+                                            int (&bw)[2][8]) {
+  const int wa = w0 + t, wb = w0 + 4 + t;
+  const bool va = wa < W, vb = wb < W;
+  const WordRef ta = tbl[va ? wa : 0], tb = tbl[vb ? wb : 0];
+  const int sa = (int)(ta.pbk >> 56), sbw = (int)(tb.pbk >> 56);
+  const int4* pba = reinterpret_cast<const int4*>(ta.pbk & kOffMask);
+  const int4* pbb = reinterpret_cast<const int4*>(tb.pbk & kOffMask);
+  const int4* o1a = SWAP ? pba : ta.pa;
+  const int4* o1b = SWAP ? pbb : tb.pa;
+  const int4* o2a = SWAP ? ta.pa : pba;
+  const int4* o2b = SWAP ? tb.pa : pbb;
+  ld_group(o1a + (int64_t)ra * sa, va && ok_a, a[0]);
+  ld_group(o1a + (int64_t)rb * sa, va && ok_b, a[1]);
+  ld_group(o1b + (int64_t)ra * sbw, vb && ok_a, a[2]);
+  ld_group(o1b + (int64_t)rb * sbw, vb && ok_b, a[3]);
+  ld_group(o2a + (int64_t)cc * sa, va && ok_c, bw[0]);
+  ld_group(o2b + (int64_t)cc * sbw, vb && ok_c, bw[1]);
+}
+
+// 16 tile rows (r0..) x 8 tile columns (c0..) of one C block, any s <= 8
+// slices, one int32 accumulator per digit pair (exact for inner lengths up to
+// 2^19).  SWAP: tile rows are the block's columns (B side), tile columns the
+// block's rows (A side).
+template <bool SWAP>
+__device__ __forceinline__ void mixed_tile(const int4* __restrict__ pa0, const int4* __restrict__ pb0, int s,
                                            const Ent* __restrict__ ent, int64_t s0, int n, int cap,
                                            WordRef* __restrict__ tbl, int TM, int TN, int r0, int c0,
                                            double (&out)[4]) {
@@ -194,7 +248,6 @@ __device__ __forceinline__ void mixed_tile(const int* __restrict__ pa0, const in
 #pragma unroll
   for (int h = 0; h < 4; ++h) out[h] = 0.0;
   for (int p = 0; p < s; ++p) {
-    const int nq = s - p;  // q = 0 .. s-1-p  (p + q <= s - 1 in 0-based digits)
     int acc[kMaxSlices][4];
 #pragma unroll
     for (int q = 0; q < kMaxSlices; ++q)
@@ -204,37 +257,24 @@ __device__ __forceinline__ void mixed_tile(const int* __restrict__ pa0, const in
       const int m = min(cap, n - base);
       const int W = build_words(pa0, pb0, ent, s0 + base, m, tbl, lane);
       for (int w0 = 0; w0 < W; w0 += 8) {
+        int aw[4][8], bw[2][8];
+        load_window<SWAP>(tbl, W, w0, t, ra, rb, cc, ok_a, ok_b, ok_c, aw, bw);
         int a[4];
-        int bq[2];
-        const int wa = w0 + t, wb = w0 + 4 + t;
-        const bool va = wa < W, vb = wb < W;
-        const WordRef ta = tbl[va ? wa : 0], tb = tbl[vb ? wb : 0];
-        const int sa = (int)(ta.pbk >> 56), sbw = (int)(tb.pbk >> 56);
-        const int* pba = reinterpret_cast<const int*>(ta.pbk & kOffMask);
-        const int* pbb = reinterpret_cast<const int*>(tb.pbk & kOffMask);
-        // tile op1 = A rows (or B columns when SWAP), plane p
-        const int* o1a = SWAP ? pba + (int64_t)p * b_plane_w : ta.pa + (int64_t)p * a_plane_w;
-        const int* o1b = SWAP ? pbb + (int64_t)p * b_plane_w : tb.pa + (int64_t)p * a_plane_w;
-        a[0] = (va && ok_a) ? __ldg(o1a + (int64_t)ra * sa) : 0;
-        a[1] = (va && ok_b) ? __ldg(o1a + (int64_t)rb * sa) : 0;
-        a[2] = (vb && ok_a) ? __ldg(o1b + (int64_t)ra * sbw) : 0;
-        a[3] = (vb && ok_b) ? __ldg(o1b + (int64_t)rb * sbw) : 0;
 #pragma unroll
-        for (int q = 0; q < kMaxSlices; ++q) {
-          if (q < nq) {
-            const int* o2a = SWAP ? ta.pa + (int64_t)q * a_plane_w : pba + (int64_t)q * b_plane_w;
-            const int* o2b = SWAP ? tb.pa + (int64_t)q * a_plane_w : pbb + (int64_t)q * b_plane_w;
-            bq[0] = (va && ok_c) ? __ldg(o2a + (int64_t)cc * sa) : 0;
-            bq[1] = (vb && ok_c) ? __ldg(o2b + (int64_t)cc * sbw) : 0;
+        for (int pp = 0; pp < kMaxSlices; ++pp)
+          if (pp == p) { a[0] = aw[0][pp]; a[1] = aw[1][pp]; a[2] = aw[2][pp]; a[3] = aw[3][pp]; }
+#pragma unroll
+        for (int q = 0; q < kMaxSlices; ++q)
+          if (q < s - p) {
+            const int bq[2] = {bw[0][q], bw[1][q]};
             imma16832(acc[q], a, bq);
           }
-        }
       }
       __syncwarp();
     }
 #pragma unroll
     for (int q = 0; q < kMaxSlices; ++q)
-      if (q < nq) {
+      if (q < s - p) {
         const int sh = -12 - 7 * (p + q);
 #pragma unroll
         for (int h = 0; h < 4; ++h) out[h] += ldexp((double)acc[q][h], sh);
@@ -247,12 +287,13 @@ __device__ __forceinline__ void mixed_tile(const int* __restrict__ pa0, const in
 // at most S products of |digit| <= 64 per inner index, so it stays exact while
 // the tile's inner length is at most (2^31 - 1) / (S * 4096) (74,898 for
 // S = 7); callers check that bound.  Per window of 8 words every plane of
-// both operands is loaded once and all S(S+1)/2 pairs run.
+// both operands is loaded once (12 16-byte loads per lane) and all
+// S(S+1)/2 pairs run.
 template <int S, bool SWAP>
-__device__ __forceinline__ void mixed_tile_levels(const int* __restrict__ pa0, const int* __restrict__ pb0,
-                                                  int64_t a_plane_w, int64_t b_plane_w, const Ent* __restrict__ ent,
-                                                  int64_t s0, int n, int cap, WordRef* __restrict__ tbl, int TM,
-                                                  int TN, int r0, int c0, double (&out)[4]) {
+__device__ __forceinline__ void mixed_tile_levels(const int4* __restrict__ pa0, const int4* __restrict__ pb0,
+                                                  const Ent* __restrict__ ent, int64_t s0, int n, int cap,
+                                                  WordRef* __restrict__ tbl, int TM, int TN, int r0, int c0,
+                                                  double (&out)[4]) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   const int ra = r0 + g, rb = r0 + g + 8, cc = c0 + g;
@@ -266,31 +307,17 @@ __device__ __forceinline__ void mixed_tile_levels(const int* __restrict__ pa0, c
     const int m = min(cap, n - base);
     const int W = build_words(pa0, pb0, ent, s0 + base, m, tbl, lane);
     for (int w0 = 0; w0 < W; w0 += 8) {
-      const int wa = w0 + t, wb = w0 + 4 + t;
-      const bool va = wa < W, vb = wb < W;
-      const WordRef ta = tbl[va ? wa : 0], tb = tbl[vb ? wb : 0];
-      const int sa = (int)(ta.pbk >> 56), sbw = (int)(tb.pbk >> 56);
-      const int* pba = reinterpret_cast<const int*>(ta.pbk & kOffMask);
-      const int* pbb = reinterpret_cast<const int*>(tb.pbk & kOffMask);
-      int a[S][4], bq[S][2];
+      int aw[4][8], bw[2][8];
+      load_window<SWAP>(tbl, W, w0, t, ra, rb, cc, ok_a, ok_b, ok_c, aw, bw);
 #pragma unroll
       for (int p = 0; p < S; ++p) {
-        // tile op1 (A rows; B columns when SWAP) and tile op2, digit plane p
-        const int* o1a = SWAP ? pba + (int64_t)p * b_plane_w : ta.pa + (int64_t)p * a_plane_w;
-        const int* o1b = SWAP ? pbb + (int64_t)p * b_plane_w : tb.pa + (int64_t)p * a_plane_w;
-        const int* o2a = SWAP ? ta.pa + (int64_t)p * a_plane_w : pba + (int64_t)p * b_plane_w;
-        const int* o2b = SWAP ? tb.pa + (int64_t)p * a_plane_w : pbb + (int64_t)p * b_plane_w;
-        a[p][0] = (va && ok_a) ? __ldg(o1a + (int64_t)ra * sa) : 0;
-        a[p][1] = (va && ok_b) ? __ldg(o1a + (int64_t)rb * sa) : 0;
-        a[p][2] = (vb && ok_a) ? __ldg(o1b + (int64_t)ra * sbw) : 0;
-        a[p][3] = (vb && ok_b) ? __ldg(o1b + (int64_t)rb * sbw) : 0;
-        bq[p][0] = (va && ok_c) ? __ldg(o2a + (int64_t)cc * sa) : 0;
-        bq[p][1] = (vb && ok_c) ? __ldg(o2b + (int64_t)cc * sbw) : 0;
+        const int a[4] = {aw[0][p], aw[1][p], aw[2][p], aw[3][p]};
+#pragma unroll
+        for (int q = 0; q < S - p; ++q) {
+          const int bq[2] = {bw[0][q], bw[1][q]};
+          imma16832(acc[p + q], a, bq);
+        }
       }
-#pragma unroll
-      for (int p = 0; p < S; ++p)
-#pragma unroll
-        for (int q = 0; q < S - p; ++q) imma16832(acc[p + q], a[p], bq[q]);
     }
     __syncwarp();
   }
@@ -306,7 +333,7 @@ __device__ __forceinline__ void mixed_tile_levels(const int* __restrict__ pa0, c
 __global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
     int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
     const int32_t* __restrict__ c_row, const int32_t* __restrict__ c_col, const Ent* __restrict__ ent,
-    const int* __restrict__ pa0, const int* __restrict__ pb0, int64_t a_plane_w, int64_t b_plane_w, int s,
+    const int4* __restrict__ pa0, const int4* __restrict__ pb0, int s,
     const int64_t* __restrict__ rbase, const int64_t* __restrict__ cbase, const int* __restrict__ ea,
     const int* __restrict__ eb, double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_words,
     int kmax4, unsigned long long* __restrict__ head) {
@@ -335,13 +362,13 @@ __global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
         double o[4];
         if (s == 7 && (int64_t)n * kmax4 <= kLevelInnerMax7) {
           if (swap)
-            mixed_tile_levels<7, true>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+            mixed_tile_levels<7, true>(pa0, pb0, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
           else
-            mixed_tile_levels<7, false>(pa0, pb0, a_plane_w, b_plane_w, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+            mixed_tile_levels<7, false>(pa0, pb0, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
         } else if (swap) {
-          mixed_tile<true>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+          mixed_tile<true>(pa0, pb0, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
         } else {
-          mixed_tile<false>(pa0, pb0, a_plane_w, b_plane_w, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
+          mixed_tile<false>(pa0, pb0, s, ent, s0, n, cap, tbl, TM, TN, r0, c0, o);
         }
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
@@ -419,18 +446,19 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
   LAMB_TRY(plane(B, 0, mp->b_soff, &mp->b_plane));
   dfree(ctx, sz);
   trace_mark(ctx, "plane sizes");
-  LAMB_TRY(scratch(ctx, kScrPlaneA, mp->a_plane * s, &mp->a_planes));
-  LAMB_TRY(scratch(ctx, kScrPlaneB, mp->b_plane * s, &mp->b_planes));
+  // 8 interleaved planes (those >= s are zero): 8 bytes per element
+  LAMB_TRY(scratch(ctx, kScrPlaneA, mp->a_plane * kMaxSlices, &mp->a_planes));
+  LAMB_TRY(scratch(ctx, kScrPlaneB, mp->b_plane * kMaxSlices, &mp->b_planes));
   if (A->nnz) {
     k_digits<<<grid_for((int64_t)A->n_rows * 32), kThreads, 0, ctx->stream>>>(
         A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, mp->rbase, nullptr, mp->ea, nullptr, 1,
-        mp->a_soff, mp->a_plane, s, mp->a_planes);
+        mp->a_soff, s, mp->a_planes);
     LAMB_LAUNCHED(ctx);
   }
   if (B->nnz) {
     k_digits<<<grid_for((int64_t)B->n_rows * 32), kThreads, 0, ctx->stream>>>(
         B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, nullptr, mp->cbase, nullptr, mp->eb, 0,
-        mp->b_soff, mp->b_plane, s, mp->b_planes);
+        mp->b_soff, s, mp->b_planes);
     LAMB_LAUNCHED(ctx);
   }
   return LAMB_GPU_OK;
@@ -479,8 +507,8 @@ int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const 
   LAMB_TRY(dalloc(ctx, &head, 1));
   LAMB_CUDA(ctx, cudaMemsetAsync(head, 0, sizeof(unsigned long long), ctx->stream));
   k_mixed<<<grid, kMixWarps * 32, smem, ctx->stream>>>(
-      sym.c_nnz, work, work_c, sym.c_row, C->col, sym.ent, reinterpret_cast<const int*>(mp.a_planes),
-      reinterpret_cast<const int*>(mp.b_planes), mp.a_plane / 4, mp.b_plane / 4, mp.s, mp.rbase, mp.cbase, mp.ea,
+      sym.c_nnz, work, work_c, sym.c_row, C->col, sym.ent, reinterpret_cast<const int4*>(mp.a_planes),
+      reinterpret_cast<const int4*>(mp.b_planes), mp.s, mp.rbase, mp.cbase, mp.ea,
       mp.eb, C->data, c_nrm, cap, tbl_words, 4 * wpe, head);
   LAMB_LAUNCHED(ctx);
   dfree(ctx, head);
