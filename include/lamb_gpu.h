@@ -238,6 +238,27 @@ LAMB_API int32_t lamb_gpu_matrix_query(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle
 LAMB_API int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, lamb_c_sector_out* out,
                                  int32_t n_sectors);
 
+/* ---- goods messages (one sector on the wire) --------------------------------- */
+/* The message lamb_goods_X_create packs for the sector exchange
+ * (src/lamb_goods_X_types.F90:79-268) and lamb_goods_X_unpack reads
+ * (src/lamb_goods_X_methods.F90:166-218): an int64 index (12 1-based
+ * (offset, size) slots for index, data, row_p, col_i, extents, flags; then
+ * row_p, col_i as int16 four to a word, extents, zero flags; each section at
+ * least one word) and the sector's float64 data store.  row_p carries all
+ * n_rows + 1 offsets.  Buffers may be host or device memory, so a message can
+ * go from one GPU's memory to another's (NCCL or peer copies) or through the
+ * host.  `sector` counts in lamb_gpu_matrix_query order. */
+LAMB_API int32_t lamb_gpu_goods_size(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, int32_t sector, int64_t* index_words,
+                                     int64_t* data_len);
+LAMB_API int32_t lamb_gpu_goods_pack(lamb_gpu_ctx* ctx, lamb_gpu_matrix handle, int32_t sector, int64_t* index,
+                                     double* data);
+/* A received message as a device matrix of one sector (subset positions 1,1);
+ * the receiver supplies what the message does not carry: its column count
+ * and the row and column block sizes. */
+LAMB_API int32_t lamb_gpu_goods_unpack(lamb_gpu_ctx* ctx, const int64_t* index, int64_t index_words,
+                                       const double* data, int32_t n_cols, const int8_t* row_blk_sizes,
+                                       const int8_t* col_blk_sizes, lamb_gpu_matrix* handle);
+
 /* ---- multiplication -------------------------------------------------------- */
 /* C := A . B (or C += A . B with LAMB_GPU_ACCUMULATE) over all sector triples
  * (A(m,k), B(k,n)) -> C(m,n); replaces lamb_multiply

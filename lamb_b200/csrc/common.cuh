@@ -165,6 +165,18 @@ int32_t upload_block_sizes(Ctx* ctx, DevMatrix* m);
 // rsub_base[a]*S + n*rsub_cnt[a] + rank.
 int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of, bool by_order = false,
                             std::vector<int64_t>* h_base = nullptr);
+// Per-sector download index of m on the device: for sector s (query order)
+// its blocks occupy [first_s, first_s + sec_nblk[s]) of col16 (1-based int16
+// columns) and ext (1-based inclusive extents into the sector's data); h_bcnt
+// (filled once the stream reaches it) holds the run length of every
+// (row subset a, column subset n, local row l) at rsub_base[a]*S + n*rsub_cnt[a] + l.
+struct SectorIndex {
+  int16_t* col16 = nullptr;
+  int64_t* ext = nullptr;
+  std::vector<int64_t> h_bcnt;
+};
+int32_t build_sector_index(Ctx* ctx, const DevMatrix* m, SectorIndex* si);
+void free_sector_index(Ctx* ctx, SectorIndex* si);
 // Exclusive scan of int64 (in place allowed), via CUB with stream-ordered scratch.
 int32_t exclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int32_t inclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);

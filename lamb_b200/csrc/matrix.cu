@@ -314,6 +314,43 @@ __global__ void k_sector_index(int32_t n_rows, int32_t n_rsub, int32_t S, const 
   }
 }
 
+int32_t build_sector_index(Ctx* ctx, const DevMatrix* m, SectorIndex* si) {
+  const int S = m->n_csub;
+  const int64_t n_seq = (int64_t)m->n_rows * S;
+  si->h_bcnt.assign(std::max<int64_t>(n_seq, 1), 0);
+  if (n_seq == 0 || m->nnz == 0) return LAMB_GPU_OK;
+  int64_t *d_dsz = nullptr, *d_bcnt = nullptr, *d_bpos = nullptr, *d_sbase = nullptr;
+  int32_t *d_rb = nullptr, *d_cb = nullptr;
+  LAMB_TRY(dalloc(ctx, &si->col16, m->nnz));
+  LAMB_TRY(dalloc(ctx, &si->ext, 2 * m->nnz));
+  LAMB_TRY(dalloc(ctx, &d_dsz, n_seq));
+  LAMB_TRY(dalloc(ctx, &d_bcnt, n_seq));
+  LAMB_TRY(dalloc(ctx, &d_bpos, n_seq));
+  LAMB_TRY(dalloc(ctx, &d_sbase, (int64_t)m->sec_base.size()));
+  LAMB_TRY(dalloc(ctx, &d_rb, m->n_rsub + 1));
+  LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
+  // the host vectors copied from are members of m: they outlive the copies
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_sbase, m->sec_base.data(), sizeof(int64_t) * m->sec_base.size(), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
+  k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+                                                                    m->col, m->row_bs, m->col_bs, nullptr, d_dsz, d_bcnt);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, d_bcnt, d_bpos, n_seq));
+  k_sector_index<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+                                                                      m->col, m->off, m->row_bs, m->col_bs, d_bpos,
+                                                                      d_sbase, si->col16, si->ext);
+  LAMB_LAUNCHED(ctx);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(si->h_bcnt.data(), d_bcnt, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
+  dfree(ctx, d_dsz); dfree(ctx, d_bcnt); dfree(ctx, d_bpos); dfree(ctx, d_sbase); dfree(ctx, d_rb); dfree(ctx, d_cb);
+  return LAMB_GPU_OK;
+}
+
+void free_sector_index(Ctx* ctx, SectorIndex* si) {
+  dfree(ctx, si->col16);
+  dfree(ctx, si->ext);
+}
+
 int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of, bool by_order, std::vector<int64_t>* h_base_out) {
   const int S = m->n_csub;
   const int64_t n_seq = (int64_t)m->n_rows * S;
@@ -665,7 +702,7 @@ int32_t lamb_gpu_matrix_upload(lamb_gpu_ctx* c, const lamb_c_sector* sec, int32_
   for (size_t k = 0; k < sid.size(); ++k)
     if (sid[k] >= 0 && sec[sid[k]].data_len > 0)
       LAMB_CUDA(ctx, cudaMemcpyAsync(m->data + m->sec_base[k], sec[sid[k]].data, sizeof(double) * sec[sid[k]].data_len,
-                                     cudaMemcpyHostToDevice, ctx->stream));
+                                     cudaMemcpyDefault, ctx->stream));
   std::vector<int64_t> h_row_p(m->n_rows + 1, 0), h_off(nnz);
   std::vector<int32_t> h_col(nnz);
   int64_t p = 0;
@@ -833,51 +870,22 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
   }
   // Sector indices (1-based int16 columns, 1-based extents) are built on the
   // device in one array ordered sector by sector, then copied per sector.
-  const int64_t n_seq = (int64_t)m->n_rows * S;
-  std::vector<int64_t> h_bcnt(std::max<int64_t>(n_seq, 1), 0);
-  int16_t* d_col16 = nullptr;
-  int64_t *d_ext = nullptr, *d_dsz = nullptr, *d_bcnt = nullptr, *d_bpos = nullptr, *d_sbase = nullptr;
-  int32_t *d_rb = nullptr, *d_cb = nullptr;
-  struct Tmp {
-    Ctx* c;
-    std::vector<void**> ps;
-    ~Tmp() { for (void** p : ps) if (*p) { cudaFreeAsync(*p, c->stream); *p = nullptr; } }
-  } tmp{ctx, {(void**)&d_col16, (void**)&d_ext, (void**)&d_dsz, (void**)&d_bcnt, (void**)&d_bpos, (void**)&d_sbase,
-              (void**)&d_rb, (void**)&d_cb}};
-  if (n_seq > 0 && m->nnz > 0) {
-    LAMB_TRY(dalloc(ctx, &d_col16, m->nnz));
-    LAMB_TRY(dalloc(ctx, &d_ext, 2 * m->nnz));
-    LAMB_TRY(dalloc(ctx, &d_dsz, n_seq));
-    LAMB_TRY(dalloc(ctx, &d_bcnt, n_seq));
-    LAMB_TRY(dalloc(ctx, &d_bpos, n_seq));
-    LAMB_TRY(dalloc(ctx, &d_sbase, (int64_t)m->sec_base.size()));
-    LAMB_TRY(dalloc(ctx, &d_rb, m->n_rsub + 1));
-    LAMB_TRY(dalloc(ctx, &d_cb, S + 1));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(d_sbase, m->sec_base.data(), sizeof(int64_t) * m->sec_base.size(), cudaMemcpyHostToDevice, ctx->stream));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
-    k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
-                                                                      m->col, m->row_bs, m->col_bs, nullptr, d_dsz,
-                                                                      d_bcnt);
-    LAMB_LAUNCHED(ctx);
-    LAMB_TRY(exclusive_scan_i64(ctx, d_bcnt, d_bpos, n_seq));
-    k_sector_index<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
-                                                                        m->col, m->off, m->row_bs, m->col_bs, d_bpos,
-                                                                        d_sbase, d_col16, d_ext);
-    LAMB_LAUNCHED(ctx);
-    LAMB_CUDA(ctx, cudaMemcpyAsync(h_bcnt.data(), d_bcnt, sizeof(int64_t) * n_seq, cudaMemcpyDeviceToHost, ctx->stream));
+  SectorIndex si;
+  LAMB_TRY(build_sector_index(ctx, m, &si));
+  {
     int64_t first = 0;
-    for (size_t s = 0; s < (size_t)m->n_rsub * S; ++s) {
+    for (size_t s = 0; s < n_sec; ++s) {
       const int64_t nb = m->sec_nblk[s];
       if (nb) {
-        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].col_i, d_col16 + first, sizeof(int16_t) * nb, cudaMemcpyDeviceToHost, ctx->stream));
-        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].extents, d_ext + 2 * first, sizeof(int64_t) * 2 * nb, cudaMemcpyDeviceToHost, ctx->stream));
+        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].col_i, si.col16 + first, sizeof(int16_t) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+        LAMB_CUDA(ctx, cudaMemcpyAsync(out[s].extents, si.ext + 2 * first, sizeof(int64_t) * 2 * nb, cudaMemcpyDeviceToHost, ctx->stream));
       }
       first += nb;
     }
   }
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->copy_stream));
+  free_sector_index(ctx, &si);
   for (int a = 0; a < m->n_rsub; ++a)
     for (int b = 0; b < S; ++b) {
       auto& o = out[a * S + b];
@@ -892,7 +900,7 @@ int32_t lamb_gpu_matrix_download(lamb_gpu_ctx* c, lamb_gpu_matrix h, lamb_c_sect
       const int64_t cnt = m->rsub_cnt[a];
       const int64_t base = (int64_t)m->rsub_base[a] * S + b * cnt;
       o.row_p[0] = 0;
-      for (int64_t l = 0; l < cnt; ++l) o.row_p[l + 1] = o.row_p[l] + (m->nnz ? h_bcnt[base + l] : 0);
+      for (int64_t l = 0; l < cnt; ++l) o.row_p[l + 1] = o.row_p[l] + (m->nnz ? si.h_bcnt[base + l] : 0);
       o.n_blks = m->sec_nblk[s];
       o.data_len = m->sec_dlen[s];
     }

@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
             "lamb_gpu_ctx_synchronize": [vp],
             "lamb_gpu_matrix_upload": [vp, P(CSector), i32, P(i64)],
             "lamb_gpu_matrix_from_coo": [vp, i32, i32, vp, vp, vp, vp, i64, vp, vp, vp, vp, i64, P(i64)],
+            "lamb_gpu_goods_size": [vp, i64, i32, P(i64), P(i64)],
+            "lamb_gpu_goods_pack": [vp, i64, i32, vp, vp],
+            "lamb_gpu_goods_unpack": [vp, vp, i64, vp, i32, vp, vp, P(i64)],
             "lamb_gpu_matrix_load_dbcsr": [vp, C.c_char_p, vp, i32, P(i64)],
             "lamb_dbcsr_scan": [C.c_char_p, P(DbcsrInfo), C.c_char_p, i32],
             "lamb_dbcsr_read": [C.c_char_p, vp, vp, vp, vp, vp, vp, i64, C.c_char_p, i32],
@@ -192,6 +195,25 @@ class Context:
         h = C.c_int64()
         self.check(lib().lamb_gpu_matrix_load_dbcsr(self._h, path.encode(), None if x is None else x.ctypes.data,
                                                     n_x_cubes, C.byref(h)))
+        return DeviceMatrix(self, h.value)
+
+    def goods_unpack(self, index, data, n_cols: int, row_blk_sizes, col_blk_sizes) -> "DeviceMatrix":
+        """A goods message (numpy arrays or CUDA tensors) as a one-sector device
+        matrix (lamb_gpu_goods_unpack)."""
+        def ptr(x):
+            if hasattr(x, "data_ptr"):
+                return x.data_ptr() if x.numel() else None
+            return x.ctypes.data if x.size else None
+        n_idx = int(index.numel() if hasattr(index, "numel") else index.size)
+        rbs = np.ascontiguousarray(row_blk_sizes, np.int8)
+        cbs = np.ascontiguousarray(col_blk_sizes, np.int8)
+        if hasattr(index, "data_ptr") and index.is_cuda:
+            import torch
+            torch.cuda.synchronize(index.device)
+        h = C.c_int64()
+        self.check(lib().lamb_gpu_goods_unpack(self._h, ptr(index), n_idx, ptr(data), n_cols,
+                                               rbs.ctypes.data if rbs.size else None,
+                                               cbs.ctypes.data if cbs.size else None, C.byref(h)))
         return DeviceMatrix(self, h.value)
 
     def create_like(self, like: "DeviceMatrix") -> "DeviceMatrix":
@@ -337,6 +359,26 @@ class DeviceMatrix:
                 secs[i] = Sector(s.subset_row, s.subset_col, s.row_blk_sizes, s.col_blk_sizes, s.row_p,
                                  s.col_i[:nb], s.extents[:nb], s.data)
         return LambMatrix(secs, "C")
+
+    def goods(self, sector: int, device: bool = False):
+        """One sector as a goods message (lamb_gpu_goods_pack): (index int64,
+        data float64) as numpy arrays, or as CUDA tensors when device=True."""
+        nw, nd = C.c_int64(), C.c_int64()
+        self.ctx.check(lib().lamb_gpu_goods_size(self.ctx.handle, self.h, sector, C.byref(nw), C.byref(nd)))
+        if device:
+            import torch
+            dev = torch.device("cuda", self.ctx.device)
+            idx = torch.empty(nw.value, dtype=torch.int64, device=dev)
+            dat = torch.empty(max(nd.value, 1), dtype=torch.float64, device=dev)[:nd.value]
+            torch.cuda.synchronize(dev)
+            self.ctx.check(lib().lamb_gpu_goods_pack(self.ctx.handle, self.h, sector, idx.data_ptr(),
+                                                     dat.data_ptr() if nd.value else None))
+            return idx, dat
+        idx = np.empty(nw.value, np.int64)
+        dat = np.empty(nd.value, np.float64)
+        self.ctx.check(lib().lamb_gpu_goods_pack(self.ctx.handle, self.h, sector, idx.ctypes.data,
+                                                 dat.ctypes.data if nd.value else None))
+        return idx, dat
 
     def set_positions(self, xyz: np.ndarray, box) -> None:
         """Row-atom coordinates in sector order (locality hint for the multiply)."""
