@@ -384,6 +384,9 @@ def run_ours(args):
             "max_rel_err_vs_oracle": err,
             "mixed": mixed,
             "stats": {k: stats[-1][k] for k in ("n_products", "n_c_blocks", "ms_symbolic", "ms_numeric", "ms_total")},
+            # timed region per step minus the multiply's own device time: host-side
+            # stalls between and inside the multiplies (the GPU idles meanwhile)
+            "host_gap_ms_per_step": ms_max / args.steps - ms_tot,
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "clocks": clocks,
         }
