@@ -330,7 +330,9 @@ __device__ __forceinline__ void mixed_tile_levels(const int4* __restrict__ pa0, 
   }
 }
 
-__global__ void __launch_bounds__(kMixWarps * 32) k_mixed(
+// Five CTAs per SM (96 registers a thread, a small spill) run the 6,144-water
+// multiply 1.8 % faster than the 128-register build at four.
+__global__ void __launch_bounds__(kMixWarps * 32, 5) k_mixed(
     int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
     const int32_t* __restrict__ c_row, const int32_t* __restrict__ c_col, const Ent* __restrict__ ent,
     const int4* __restrict__ pa0, const int4* __restrict__ pb0, int s,
