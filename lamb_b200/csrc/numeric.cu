@@ -33,6 +33,14 @@ namespace lamb {
 constexpr int kNumWarps = 8;
 constexpr int kMaxChunk = 32;
 
+// Consecutive work items a warp takes per queue fetch (LAMB_GPU_GRAB, 1-64;
+// default 1).
+static int stacked_grab() {
+  const char* v = getenv("LAMB_GPU_GRAB");
+  const int g = v ? atoi(v) : 1;
+  return std::max(1, std::min(g, 64));
+}
+
 // Column table entry: pointers to op1(0,kk) and op2(kk,0); the runtime
 // stride (the entry's inner block size) sits in the top byte of `pbk`.
 struct ColRef {
@@ -292,16 +300,18 @@ __global__ void __launch_bounds__(kNumWarps * 32, 3)
     k_stacked(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
               const Ent* __restrict__ ent, const double* __restrict__ d1, const double* __restrict__ d2,
               double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_cols,
-              unsigned long long* __restrict__ head) {
+              unsigned long long* __restrict__ head, int grab) {
   extern __shared__ ColRef tbl_all[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ColRef* tbl = tbl_all + (size_t)w * tbl_cols;
   while (true) {
-    unsigned long long v = 0;
-    if (lane == 0) v = atomicAdd(head, 1ull);
-    v = __shfl_sync(0xffffffffu, v, 0);
-    if (v >= (unsigned long long)n_work) break;
-    process_item<TA, TB>(work[v], work_c[v], ent, d1, d2, out, out_nrm, tbl, cap);
+    unsigned long long start = 0;
+    if (lane == 0) start = atomicAdd(head, (unsigned long long)grab);
+    start = __shfl_sync(0xffffffffu, start, 0);
+    if (start >= (unsigned long long)n_work) break;
+    const int64_t end = min((int64_t)start + grab, n_work);
+    for (int64_t v = (int64_t)start; v < end; ++v)
+      process_item<TA, TB>(work[v], work_c[v], ent, d1, d2, out, out_nrm, tbl, cap);
   }
 }
 
@@ -329,12 +339,24 @@ __global__ void __launch_bounds__(NW * 32, 24 / NW)
   }
 }
 
+// Stack entries per column-table chunk: at most `want`, and few enough that
+// the tables of `warps` warps (cap x max_inner columns each) fit the device's
+// opt-in shared memory per CTA (227 KB on B200; blocks of 127 rows allow 14
+// entries per chunk).
+static int table_cap(Ctx* ctx, int want, int max_inner, int warps) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess || optin <= 0)
+    optin = 48 * 1024;
+  const int fit = optin / (int)(sizeof(ColRef) * (size_t)max_inner * warps);
+  return std::max(1, std::min(want, std::min(8192 / max_inner, fit)));
+}
+
 template <int NW>
 static int32_t launch_batch_nw(Ctx* ctx, int64_t n_work, const Work* work, const int32_t* work_c,
                                const int32_t* work_i, const BatchInst* inst, unsigned long long* head, int grab,
                                int cap, int max_inner) {
   const int mi = std::max(1, std::min(max_inner, 127));
-  cap = std::max(1, std::min(cap, 8192 / mi));
+  cap = table_cap(ctx, cap, mi, NW);
   const int tbl_cols = cap * mi;
   const size_t smem = sizeof(ColRef) * (size_t)tbl_cols * NW;
   auto kern = k_stacked_batch<NW>;
@@ -361,7 +383,7 @@ static int32_t launch_stacked(Ctx* ctx, int64_t n_work, const Work* work, const 
                               const double* d1, const double* d2, double* out, double* out_nrm, int max_inner) {
   // Column table per warp: `cap` entries of up to max_inner columns each.
   const int mi = std::max(1, std::min(max_inner, 127));
-  int cap = std::max(1, std::min(kMaxChunk, 8192 / mi));
+  const int cap = table_cap(ctx, kMaxChunk, mi, kNumWarps);
   const int tbl_cols = cap * mi;
   const size_t smem = sizeof(ColRef) * (size_t)tbl_cols * kNumWarps;
   auto kern = k_stacked<TA, TB>;
@@ -375,7 +397,8 @@ static int32_t launch_stacked(Ctx* ctx, int64_t n_work, const Work* work, const 
   unsigned long long* head = nullptr;
   LAMB_TRY(dalloc(ctx, &head, 1));
   LAMB_CUDA(ctx, cudaMemsetAsync(head, 0, sizeof(unsigned long long), ctx->stream));
-  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols, head);
+  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols, head,
+                                                    stacked_grab());
   LAMB_LAUNCHED(ctx);
   dfree(ctx, head);
   return LAMB_GPU_OK;

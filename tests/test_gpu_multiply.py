@@ -75,6 +75,50 @@ def test_empty_and_tiny(gpu_ctx):
     assert_same_pattern(c, c_ref)
 
 
+def _sector_from_blocks(rb, cb, blocks, rng):
+    """One sector (1, 1) whose blocks, given as 1-based (row, col) keys, get random values."""
+    rows = sorted(blocks)
+    row_p = np.zeros(len(rb) + 1, np.int64)
+    col_i, ext, data, pos = [], [], [], 1
+    for r, c in rows:
+        row_p[r] += 1
+        n = int(rb[r - 1]) * int(cb[c - 1])
+        col_i.append(c)
+        ext.append((pos, pos + n - 1))
+        data.append(rng.standard_normal(n))
+        pos += n
+    row_p = np.concatenate([[0], np.cumsum(row_p[1:])]).astype(np.int64)
+    return Sector(1, 1, np.asarray(rb, np.int8), np.asarray(cb, np.int8), row_p, np.asarray(col_i, np.int16),
+                  np.asarray(ext, np.int64).reshape(-1, 2), np.concatenate(data) if data else np.zeros(0))
+
+
+def test_largest_local_index_and_block_size(gpu_ctx):
+    """A subset of 32767 atoms (the largest 1-based int16 local column) and
+    127-row blocks (the largest int8 block size) on the inner dimension, with a
+    zero-size row; 32768 atoms are refused at upload."""
+    rng = np.random.default_rng(11)
+    nk = 32767
+    kb = np.ones(nk, np.int8)
+    kb[0], kb[nk // 2], kb[nk - 1] = 2, 0, 127
+    ab = np.array([127, 1, 0], np.int8)
+    bb = np.array([127, 3], np.int8)
+    a = LambMatrix([_sector_from_blocks(ab, kb, {(1, 1): 0, (1, nk // 2 + 1): 0, (1, nk): 0, (2, nk): 0,
+                                                (2, 7): 0, (3, 1): 0}, rng)])
+    b = LambMatrix([_sector_from_blocks(kb, bb, {(1, 1): 0, (1, 2): 0, (7, 2): 0, (nk // 2 + 1, 1): 0,
+                                                (nk, 1): 0, (nk, 2): 0}, rng)])
+    a.validate()
+    b.validate()
+    c_ref, st_ref = oracle.multiply(a, b, 0.0)
+    c, st = _gpu_mult(gpu_ctx, a, b, 0.0)
+    assert_same_pattern(c, c_ref)
+    assert rel_frobenius_error(c, c_ref) <= TOL_FP64
+    assert st["flops"] == st_ref["flops"]
+    too_wide = LambMatrix([_sector_from_blocks(np.ones(1, np.int8), np.ones(nk + 1, np.int8), {(1, 1): 0}, rng)])
+    with pytest.raises(gpu.LambError) as ei:
+        gpu_ctx.upload(too_wide)
+    assert ei.value.type == 100 and "32767" in str(ei.value)
+
+
 @pytest.mark.parametrize("seed", [0, 5])
 def test_stacks_bit_exact(gpu_ctx, seed):
     g = WaterGeometry(48, None, 6.0, seed=seed)
