@@ -417,45 +417,8 @@ __global__ void k_order_lens(int32_t n_rows, const int32_t* __restrict__ order, 
   }
 }
 
-// rank[order[w]] = w: position of every atom in a processing order.
-__global__ void k_order_rank(int32_t n, const int32_t* __restrict__ order, int32_t* __restrict__ rank) {
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n; w += (int64_t)gridDim.x * blockDim.x)
-    rank[order[w]] = (int32_t)w;
-}
-
-// Sort keys (column rank) and values (C block) of every work item, in work order.
-__global__ void k_work_keys(int64_t n_work, const int32_t* __restrict__ work_c, const int32_t* __restrict__ col,
-                            const int32_t* __restrict__ col_rank, int32_t* __restrict__ key) {
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_work; v += (int64_t)gridDim.x * blockDim.x)
-    key[v] = col_rank[col[work_c[v]]];
-}
-
-__global__ void k_work_from_c(int64_t n_work, const int32_t* __restrict__ cs, const int32_t* __restrict__ c_row,
-                              const int32_t* __restrict__ col, const int64_t* __restrict__ off,
-                              const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs,
-                              const int64_t* __restrict__ stack_p, Work* __restrict__ work,
-                              int32_t* __restrict__ work_c) {
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_work; v += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t c = cs[v];
-    const long long bi = row_bs[c_row[c]], bj = col_bs[col[c]];
-    const long long n = stack_p[c + 1] - stack_p[c];
-    work[v] = Work{(long long)off[c] | (bi << 40) | (bj << 48), (long long)stack_p[c] | (n << 40)};
-    work_c[v] = c;
-  }
-}
-
-int32_t column_rank(Ctx* ctx, const DevMatrix* order_src, int32_t** rank) {
-  *rank = nullptr;
-  const int n = order_src->n_rows;
-  if (n == 0 || !order_src->order) return LAMB_GPU_OK;
-  LAMB_TRY(dalloc(ctx, rank, n));
-  k_order_rank<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, *rank);
-  LAMB_LAUNCHED(ctx);
-  return LAMB_GPU_OK;
-}
-
 int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
-                   int32_t** work_c, bool use_scratch, const int32_t* col_rank) {
+                   int32_t** work_c, bool use_scratch) {
   const int n = C->n_rows;
   if (use_scratch) {
     LAMB_TRY(scratch(ctx, kScrWork, sym.c_nnz, work));
@@ -478,34 +441,6 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
   k_build_work<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, d_cum, C->row_p, C->col, C->off,
                                                             C->row_bs, C->col_bs, sym.stack_p, *work, *work_c);
   LAMB_LAUNCHED(ctx);
-  if (col_rank && sym.c_row) {
-    // Inside every row, take the C blocks in the processing order of their
-    // column atoms: consecutive items then have neighbouring column atoms,
-    // whose stacks share most of their A blocks (A_ik with k near both).
-    const int64_t nw = sym.c_nnz;
-    int32_t *key_in = nullptr, *key_out = nullptr, *c_out = nullptr;
-    int64_t* seg = nullptr;
-    LAMB_TRY(dalloc(ctx, &key_in, nw));
-    LAMB_TRY(dalloc(ctx, &key_out, nw));
-    LAMB_TRY(dalloc(ctx, &c_out, nw));
-    LAMB_TRY(dalloc(ctx, &seg, (int64_t)n + 1));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(seg, d_cum, sizeof(int64_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-    LAMB_CUDA(ctx, cudaMemcpyAsync(seg + n, &sym.c_nnz, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
-    k_work_keys<<<grid_for(nw), kThreads, 0, ctx->stream>>>(nw, *work_c, C->col, col_rank, key_in);
-    LAMB_LAUNCHED(ctx);
-    size_t tmp_bytes = 0;
-    LAMB_CUDA(ctx, cub::DeviceSegmentedSort::SortPairs(nullptr, tmp_bytes, key_in, key_out, *work_c, c_out, nw, n,
-                                                        seg, seg + 1, ctx->stream));
-    void* tmp = nullptr;
-    LAMB_TRY(dalloc_bytes(ctx, &tmp, std::max<size_t>(tmp_bytes, 1)));
-    LAMB_CUDA(ctx, cub::DeviceSegmentedSort::SortPairs(tmp, tmp_bytes, key_in, key_out, *work_c, c_out, nw, n, seg,
-                                                        seg + 1, ctx->stream));
-    k_work_from_c<<<grid_for(nw), kThreads, 0, ctx->stream>>>(nw, c_out, sym.c_row, C->col, C->off, C->row_bs,
-                                                              C->col_bs, sym.stack_p, *work, *work_c);
-    LAMB_LAUNCHED(ctx);
-    cudaFreeAsync(tmp, ctx->stream);
-    dfree(ctx, key_in); dfree(ctx, key_out); dfree(ctx, c_out); dfree(ctx, seg);
-  }
   dfree(ctx, d_len);
   dfree(ctx, d_cum);
   return LAMB_GPU_OK;
@@ -704,7 +639,6 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   double* c_nrm = nullptr;
   Work* work = nullptr;
   int32_t* work_c = nullptr;
-  int32_t* col_rank = nullptr;
   int slices = 0;
   int64_t dropped = 0;
   MixedPlanes mp;
@@ -727,13 +661,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
     }
     trace_mark(ctx, "symbolic");
-    // C's columns are A's row atoms when B's column structure is A's row
-    // structure (square products over one set of atoms): then the work items
-    // of every row follow A's row processing order over their columns.
-    const char* co = getenv("LAMB_GPU_COL_ORDER");
-    if (co && atoi(co) != 0 && B->n_cols == A->n_rows && B->csub_cnt == A->rsub_cnt && B->h_col_bs == A->h_row_bs)
-      LAMB_TRY(column_rank(ctx, A, &col_rank));
-    LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c, true, col_rank));
+    LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c, true));
     LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
     trace_mark(ctx, "work items");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
@@ -752,7 +680,6 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   free_slices(ctx, &mp);
   dfree(ctx, a_offk);
   dfree(ctx, c_nrm);
-  dfree(ctx, col_rank);
   free_symbolic(ctx, sym);
   if (rc != LAMB_GPU_OK) return rc;
   C->norms_valid = false;

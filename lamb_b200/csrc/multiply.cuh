@@ -53,12 +53,8 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
                        const int64_t* a_offk, Symbolic* out, const int64_t* b_meta = nullptr);
 // Work list of C blocks in the row processing order of `order_src` (its h_order).
 // use_scratch: work and work_c come from the context's scratch (not to be freed).
-// col_rank (optional, [C columns]): position of every column atom in a
-// processing order; inside each row the work items then follow it.
 int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevMatrix* order_src, Work** work,
-                   int32_t** work_c, bool use_scratch = false, const int32_t* col_rank = nullptr);
-// Position of every row atom of order_src in its processing order (null when it has none).
-int32_t column_rank(Ctx* ctx, const DevMatrix* order_src, int32_t** rank);
+                   int32_t** work_c, bool use_scratch = false);
 // Stacked small-GEMM kernels: out_c = sum_e op1_e . op2_e over the work list.
 // TA/TB select transposed operands (used by the adjoint); see numeric.cu.
 // max_inner: the largest inner block size of any entry (sizes the column table).

@@ -33,14 +33,6 @@ namespace lamb {
 constexpr int kNumWarps = 8;
 constexpr int kMaxChunk = 32;
 
-// Consecutive work items a warp takes per queue fetch (LAMB_GPU_GRAB, 1-64;
-// default 1).
-static int stacked_grab() {
-  const char* v = getenv("LAMB_GPU_GRAB");
-  const int g = v ? atoi(v) : 1;
-  return std::max(1, std::min(g, 64));
-}
-
 // Column table entry: pointers to op1(0,kk) and op2(kk,0); the runtime
 // stride (the entry's inner block size) sits in the top byte of `pbk`.
 struct ColRef {
@@ -300,18 +292,16 @@ __global__ void __launch_bounds__(kNumWarps * 32, 3)
     k_stacked(int64_t n_work, const Work* __restrict__ work, const int32_t* __restrict__ work_c,
               const Ent* __restrict__ ent, const double* __restrict__ d1, const double* __restrict__ d2,
               double* __restrict__ out, double* __restrict__ out_nrm, int cap, int tbl_cols,
-              unsigned long long* __restrict__ head, int grab) {
+              unsigned long long* __restrict__ head) {
   extern __shared__ ColRef tbl_all[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   ColRef* tbl = tbl_all + (size_t)w * tbl_cols;
   while (true) {
-    unsigned long long start = 0;
-    if (lane == 0) start = atomicAdd(head, (unsigned long long)grab);
-    start = __shfl_sync(0xffffffffu, start, 0);
-    if (start >= (unsigned long long)n_work) break;
-    const int64_t end = min((int64_t)start + grab, n_work);
-    for (int64_t v = (int64_t)start; v < end; ++v)
-      process_item<TA, TB>(work[v], work_c[v], ent, d1, d2, out, out_nrm, tbl, cap);
+    unsigned long long v = 0;
+    if (lane == 0) v = atomicAdd(head, 1ull);
+    v = __shfl_sync(0xffffffffu, v, 0);
+    if (v >= (unsigned long long)n_work) break;
+    process_item<TA, TB>(work[v], work_c[v], ent, d1, d2, out, out_nrm, tbl, cap);
   }
 }
 
@@ -397,8 +387,7 @@ static int32_t launch_stacked(Ctx* ctx, int64_t n_work, const Work* work, const 
   unsigned long long* head = nullptr;
   LAMB_TRY(dalloc(ctx, &head, 1));
   LAMB_CUDA(ctx, cudaMemsetAsync(head, 0, sizeof(unsigned long long), ctx->stream));
-  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols, head,
-                                                    stacked_grab());
+  kern<<<grid, kNumWarps * 32, smem, ctx->stream>>>(n_work, work, work_c, ent, d1, d2, out, out_nrm, cap, tbl_cols, head);
   LAMB_LAUNCHED(ctx);
   dfree(ctx, head);
   return LAMB_GPU_OK;
