@@ -310,6 +310,10 @@ def run_ours(args):
         lib.lamb_probe_int8_tops.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
         ipeak = ctypes.c_double()
         ctx.check(lib.lamb_probe_int8_tops(local, 5, ctypes.byref(ipeak)))
+        # bf16 slices with FP32 accumulation: the alternative slice format (context only)
+        lib.lamb_probe_bf16_tflops.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+        hpeak = ctypes.c_double()
+        ctx.check(lib.lamb_probe_bf16_tflops(local, 5, ctypes.byref(hpeak)))
         s_m = int(mst[-1]["mixed_slices"])
         ms_mn = statistics.mean(s["ms_numeric"] for s in mst)
         # every FP64-equivalent flop is s(s+1)/2 int8 plane-product ops (digit pairs p + q <= s - 1)
@@ -323,7 +327,8 @@ def run_ours(args):
                  "ms_symbolic": statistics.mean(s["ms_symbolic"] for s in mst),
                  "slices": int(mst[-1]["mixed_slices"]), "steps": args.mixed_steps,
                  "rel_frobenius_err_vs_fp64": rel, "ms_ratio_vs_fp64": ms_m / ms_tot,
-                 "path": "int8 digit slices, mma.m16n8k32.s8, exact int32 planes, FP64 recombination"}
+                 "path": "int8 digit slices, mma.m16n8k32.s8, exact int32 planes, FP64 recombination",
+                 "bf16_mma_sync_peak_tflops": hpeak.value}
         dcm.destroy()
     # e2e through the C ABI with page-locked host buffers
     pa, pb = pin_matrix(a), pin_matrix(b)

@@ -1,7 +1,8 @@
 /*
  * lamb_probe.h -- measurement helper of liblamb_b200.so (not part of the
- * drop-in ABI): the FP64 and int8 tensor-pipe peaks of the current GPU, used
- * as the roofline denominators of the FP64 and the int8-slice multiplies.  No reference counterpart.
+ * drop-in ABI): the FP64, int8 and bf16 tensor-pipe peaks of the current GPU;
+ * the first two are the roofline denominators of the FP64 and the int8-slice
+ * multiplies.  No reference counterpart.
  */
 #ifndef LAMB_PROBE_H
 #define LAMB_PROBE_H
@@ -17,6 +18,10 @@ LAMB_API int32_t lamb_probe_fp64_tflops(int32_t device, int32_t reps, double* tf
  * (mma.m16n8k32.s8.s8.s32 through mma.sync); writes TOP/s (1 op = 1 multiply
  * or 1 add).  Allocates 4 bytes per thread of the grid. */
 LAMB_API int32_t lamb_probe_int8_tops(int32_t device, int32_t reps, double* tops);
+/* Same for bf16 operands with FP32 accumulation (mma.m16n8k16.f32.bf16.bf16.f32
+ * through mma.sync), the alternative slice format; writes TFLOP/s.  Allocates
+ * 4 bytes per thread of the grid. */
+LAMB_API int32_t lamb_probe_bf16_tflops(int32_t device, int32_t reps, double* tflops);
 #ifdef __cplusplus
 }
 #endif
