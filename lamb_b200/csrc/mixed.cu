@@ -233,9 +233,11 @@ __device__ __forceinline__ void load_window(const WordRef* __restrict__ tbl, int
 }
 
 // 16 tile rows (r0..) x 8 tile columns (c0..) of one C block, any s <= 8
-// slices, one int32 accumulator per digit pair (exact for inner lengths up to
-// 2^19).  SWAP: tile rows are the block's columns (B side), tile columns the
-// block's rows (A side).
+// slices, one int32 accumulator per digit pair and table chunk, added into
+// the FP64 result after every chunk (a chunk has at most 4,096 inner
+// indices; an int32 sum of |digit| <= 64 products is exact up to 2^19), so
+// stacks of any length stay exact.  SWAP: tile rows are the block's columns
+// (B side), tile columns the block's rows (A side).
 template <bool SWAP>
 __device__ __forceinline__ void mixed_tile(const int4* __restrict__ pa0, const int4* __restrict__ pb0, int s,
                                            const Ent* __restrict__ ent, int64_t s0, int n, int cap,
@@ -248,12 +250,12 @@ __device__ __forceinline__ void mixed_tile(const int4* __restrict__ pa0, const i
 #pragma unroll
   for (int h = 0; h < 4; ++h) out[h] = 0.0;
   for (int p = 0; p < s; ++p) {
-    int acc[kMaxSlices][4];
-#pragma unroll
-    for (int q = 0; q < kMaxSlices; ++q)
-#pragma unroll
-      for (int h = 0; h < 4; ++h) acc[q][h] = 0;
     for (int base = 0; base < n; base += cap) {
+      int acc[kMaxSlices][4];
+#pragma unroll
+      for (int q = 0; q < kMaxSlices; ++q)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) acc[q][h] = 0;
       const int m = min(cap, n - base);
       const int W = build_words(pa0, pb0, ent, s0 + base, m, tbl, lane);
       for (int w0 = 0; w0 < W; w0 += 8) {
@@ -271,14 +273,15 @@ __device__ __forceinline__ void mixed_tile(const int4* __restrict__ pa0, const i
           }
       }
       __syncwarp();
+      // flushed per chunk: a chunk has at most cap x 128 inner indices
+#pragma unroll
+      for (int q = 0; q < kMaxSlices; ++q)
+        if (q < s - p) {
+          const int sh = -12 - 7 * (p + q);
+#pragma unroll
+          for (int h = 0; h < 4; ++h) out[h] += ldexp((double)acc[q][h], sh);
+        }
     }
-#pragma unroll
-    for (int q = 0; q < kMaxSlices; ++q)
-      if (q < s - p) {
-        const int sh = -12 - 7 * (p + q);
-#pragma unroll
-        for (int h = 0; h < 4; ++h) out[h] += ldexp((double)acc[q][h], sh);
-      }
   }
 }
 

@@ -22,7 +22,6 @@ def _gpu_mult(ctx, a, b, eps, flags=0):
     dc = ctx.create_like(da)
     st = ctx.multiply(da, db, dc, eps, flags)
     c = dc.download()
-    stk = None
     for m in (dc, db, da):
         m.destroy()
     return c, st
@@ -117,6 +116,28 @@ def test_largest_local_index_and_block_size(gpu_ctx):
     with pytest.raises(gpu.LambError) as ei:
         gpu_ctx.upload(too_wide)
     assert ei.value.type == 100 and "32767" in str(ei.value)
+
+
+@pytest.mark.parametrize("flags", [0, gpu.MIXED])
+def test_long_stack_of_full_digits(gpu_ctx, flags):
+    """One 1 x 1 C block whose stack has 4,200 products over 127-wide inner
+    blocks (533,400 inner indices), every entry 0.999: the leading int8 digit
+    is 64 everywhere, so one int32 sum over the whole stack would exceed 2^31."""
+    rng = np.random.default_rng(3)
+    nk = 4200
+    kb = np.full(nk, 127, np.int8)
+    one = np.ones(1, np.int8)
+    a = LambMatrix([_sector_from_blocks(one, kb, {(1, k): 0 for k in range(1, nk + 1)}, rng)])
+    b = LambMatrix([_sector_from_blocks(kb, one, {(k, 1): 0 for k in range(1, nk + 1)}, rng)])
+    for m in (a, b):
+        m.sectors[0].data[:] = 0.999
+    c, st = _gpu_mult(gpu_ctx, a, b, 0.0, flags)
+    assert st["n_products"] == nk
+    assert_same_pattern(c, oracle.multiply(a, b, 0.0)[0])
+    if flags & gpu.MIXED:  # against the long-double oracle, like the other mixed tests
+        assert rel_frobenius_error(c, oracle.multiply(a, b, 0.0, oracle.LONG_DOUBLE)[0]) <= 1e-11
+    else:  # FP64 sums over 533,400 terms drift 1.5e-11 from the exact value; the oracle sums alike
+        assert rel_frobenius_error(c, oracle.multiply(a, b, 0.0)[0]) <= TOL_FP64
 
 
 @pytest.mark.parametrize("seed", [0, 5])
