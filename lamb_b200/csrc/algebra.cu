@@ -21,14 +21,14 @@ bool is_square(const DevMatrix* x) {
 }
 
 __global__ void k_expand_rows(int32_t n_rows, const int64_t* __restrict__ row_p, int32_t* __restrict__ row_of) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) row_of[b] = (int32_t)r;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps())
+    for (int64_t b = row_p[r] + (threadIdx.x & 31); b < row_p[r + 1]; b += 32) row_of[b] = (int32_t)r;
 }
 
 int32_t expand_rows(Ctx* ctx, const DevMatrix* m, int32_t** row_of) {
   LAMB_TRY(dalloc(ctx, row_of, std::max<int64_t>(m->nnz, 1)));
   if (m->nnz) {
-    k_expand_rows<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, *row_of);
+    k_expand_rows<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->row_p, *row_of);
     LAMB_LAUNCHED(ctx);
   }
   return LAMB_GPU_OK;

@@ -196,6 +196,36 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
   }
   return v;
 }
+__device__ __forceinline__ long long warp_incl_scan_ll(long long v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    long long t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// First position in [lo, hi) whose column is >= c (columns ascending within a row).
+__device__ __forceinline__ int64_t lower_col(const int32_t* __restrict__ col, int64_t lo, int64_t hi, int32_t c) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (col[mid] < c) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+// Row subset of row r (n_rsub is small: a linear scan).
+__device__ __forceinline__ int row_subset(const int32_t* __restrict__ rsub_base, int32_t n_rsub, int64_t r) {
+  int m = 0;
+  while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+  return m;
+}
+// Warp-per-row loops: global warp index and warp count of the grid.
+__device__ __forceinline__ int64_t global_warp() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+__device__ __forceinline__ int64_t grid_warps() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
 
 // Fixed-order block norm: sequential fma over the block in storage order.
 // The CPU oracle uses the same expression, so the filter decisions agree bit for bit.

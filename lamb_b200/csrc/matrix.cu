@@ -231,29 +231,25 @@ __global__ void k_part_sizes(int32_t n_rows, int32_t n_rsub, int32_t S, const in
                              const int32_t* __restrict__ col, const int8_t* __restrict__ row_bs,
                              const int8_t* __restrict__ col_bs, const int32_t* __restrict__ lrank,
                              int64_t* __restrict__ dsz, int64_t* __restrict__ bcnt) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    int m = 0;
-    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
+    const int m = row_subset(rsub_base, n_rsub, r);
     const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
     const int64_t l = lrank ? lrank[r] : r - rsub_base[m];
     const int64_t base = (int64_t)rsub_base[m] * S + l;
-    const int bi = row_bs[r];
-    int n = 0;
-    int64_t ds = 0, bc = 0;
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      const int c = col[b];
-      while (c >= csub_base[n + 1]) {
+    const long long bi = row_bs[r];
+    const int64_t b1 = row_p[r + 1];
+    int64_t lo = row_p[r];
+    for (int n = 0; n < S; ++n) {
+      const int64_t hi = lower_col(col, lo, b1, csub_base[n + 1]);
+      long long ds = 0;
+      for (int64_t b = lo + lane; b < hi; b += 32) ds += col_bs[col[b]];
+      ds = warp_sum_ll(ds) * bi;
+      if (lane == 0) {
         dsz[base + n * cnt] = ds;
-        bcnt[base + n * cnt] = bc;
-        ds = 0; bc = 0; ++n;
+        bcnt[base + n * cnt] = hi - lo;
       }
-      ds += (int64_t)bi * col_bs[c];
-      ++bc;
-    }
-    for (; n < S; ++n) {
-      dsz[base + n * cnt] = ds;
-      bcnt[base + n * cnt] = bc;
-      ds = 0; bc = 0;
+      lo = hi;
     }
   }
 }
@@ -264,21 +260,29 @@ __global__ void k_part_offsets(int32_t n_rows, int32_t n_rsub, int32_t S, const 
                                const int8_t* __restrict__ col_bs, const int64_t* __restrict__ dbase,
                                const int32_t* __restrict__ lrank, int64_t* __restrict__ off,
                                int32_t* __restrict__ row_of) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    int m = 0;
-    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
+    const int m = row_subset(rsub_base, n_rsub, r);
     const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
     const int64_t l = lrank ? lrank[r] : r - rsub_base[m];
     const int64_t base = (int64_t)rsub_base[m] * S + l;
-    const int bi = row_bs[r];
-    int n = 0;
-    int64_t o = dbase[base];
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      const int c = col[b];
-      while (c >= csub_base[n + 1]) { ++n; o = dbase[base + n * cnt]; }
-      off[b] = o;
-      o += (int64_t)bi * col_bs[c];
-      if (row_of) row_of[b] = (int32_t)r;
+    const long long bi = row_bs[r];
+    const int64_t b1 = row_p[r + 1];
+    int64_t lo = row_p[r];
+    for (int n = 0; n < S; ++n) {
+      const int64_t hi = lower_col(col, lo, b1, csub_base[n + 1]);
+      long long o = dbase[base + n * cnt];
+      for (int64_t b0 = lo; b0 < hi; b0 += 32) {
+        const int64_t b = b0 + lane;
+        const long long v = b < hi ? bi * col_bs[col[b]] : 0;
+        const long long incl = warp_incl_scan_ll(v, lane);
+        if (b < hi) {
+          off[b] = o + incl - v;
+          if (row_of) row_of[b] = (int32_t)r;
+        }
+        o += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      lo = hi;
     }
   }
 }
@@ -293,23 +297,26 @@ __global__ void k_sector_index(int32_t n_rows, int32_t n_rsub, int32_t S, const 
                                const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs,
                                const int64_t* __restrict__ bpos, const int64_t* __restrict__ sec_base,
                                int16_t* __restrict__ col16, int64_t* __restrict__ ext) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    int m = 0;
-    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
+    const int m = row_subset(rsub_base, n_rsub, r);
     const int64_t cnt = rsub_base[m + 1] - rsub_base[m];
     const int64_t l = r - rsub_base[m];
     const int64_t base = (int64_t)rsub_base[m] * S + l;
     const int64_t bi = row_bs[r];
-    int n = 0;
-    int64_t q = bpos[base];
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      const int c = col[b];
-      while (c >= csub_base[n + 1]) { ++n; q = bpos[base + n * cnt]; }
-      const int64_t e1 = off[b] - sec_base[(int64_t)m * S + n] + 1;
-      col16[q] = (int16_t)(c - csub_base[n] + 1);
-      ext[2 * q] = e1;
-      ext[2 * q + 1] = e1 + bi * col_bs[c] - 1;
-      ++q;
+    const int64_t b1 = row_p[r + 1];
+    int64_t lo = row_p[r];
+    for (int n = 0; n < S; ++n) {
+      const int64_t hi = lower_col(col, lo, b1, csub_base[n + 1]);
+      const int64_t q0 = bpos[base + n * cnt] - lo, sb = sec_base[(int64_t)m * S + n];
+      for (int64_t b = lo + lane; b < hi; b += 32) {
+        const int c = col[b];
+        const int64_t q = q0 + b, e1 = off[b] - sb + 1;
+        col16[q] = (int16_t)(c - csub_base[n] + 1);
+        ext[2 * q] = e1;
+        ext[2 * q + 1] = e1 + bi * col_bs[c] - 1;
+      }
+      lo = hi;
     }
   }
 }
@@ -333,11 +340,11 @@ int32_t build_sector_index(Ctx* ctx, const DevMatrix* m, SectorIndex* si) {
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_sbase, m->sec_base.data(), sizeof(int64_t) * m->sec_base.size(), cudaMemcpyHostToDevice, ctx->stream));
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
-  k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+  k_part_sizes<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
                                                                     m->col, m->row_bs, m->col_bs, nullptr, d_dsz, d_bcnt);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, d_bcnt, d_bpos, n_seq));
-  k_sector_index<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+  k_sector_index<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
                                                                       m->col, m->off, m->row_bs, m->col_bs, d_bpos,
                                                                       d_sbase, si->col16, si->ext);
   LAMB_LAUNCHED(ctx);
@@ -383,11 +390,11 @@ int32_t layout_sector_major(Ctx* ctx, DevMatrix* m, int32_t* row_of, bool by_ord
   }
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, m->rsub_base.data(), sizeof(int32_t) * (m->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_cb, m->csub_base.data(), sizeof(int32_t) * (S + 1), cudaMemcpyHostToDevice, ctx->stream));
-  k_part_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+  k_part_sizes<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
                                                                     m->col, m->row_bs, m->col_bs, d_rank, dsz, bcnt);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, dsz, dbase, n_seq));
-  k_part_offsets<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
+  k_part_offsets<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->n_rsub, S, d_rb, d_cb, m->row_p,
                                                                       m->col, m->row_bs, m->col_bs, dbase, d_rank,
                                                                       m->off, row_of);
   LAMB_LAUNCHED(ctx);

@@ -109,8 +109,8 @@ __global__ void k_col_exp(int32_t n_rows, const int64_t* __restrict__ row_p, con
 __global__ void k_plane_sizes(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                               const int8_t* __restrict__ row_bs, const int8_t* __restrict__ col_bs, int a_side,
                               int64_t* __restrict__ sz) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps())
+    for (int64_t b = row_p[r] + (threadIdx.x & 31); b < row_p[r + 1]; b += 32) {
       const int rb = row_bs[r], cb = col_bs[col[b]];
       sz[b] = a_side ? (int64_t)rb * pad4(cb) : (int64_t)cb * pad4(rb);
     }
@@ -437,7 +437,7 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
   auto plane = [&](const DevMatrix* m, int a_side, int64_t* soff, int64_t* bytes) -> int32_t {
     LAMB_CUDA(ctx, cudaMemsetAsync(sz + m->nnz, 0, sizeof(int64_t), ctx->stream));
     if (m->nnz) {
-      k_plane_sizes<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->row_bs,
+      k_plane_sizes<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->row_bs,
                                                                          m->col_bs, a_side, sz);
       LAMB_LAUNCHED(ctx);
     }
@@ -479,14 +479,15 @@ void free_slices(Ctx* ctx, MixedPlanes* mp) {
 __global__ void k_pack_plane_meta(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                                   const int8_t* __restrict__ col_bs, const int64_t* __restrict__ soff,
                                   int64_t* __restrict__ out) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) out[b] = soff[b] | ((int64_t)col_bs[col[b]] << 56);
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps())
+    for (int64_t b = row_p[r] + (threadIdx.x & 31); b < row_p[r + 1]; b += 32)
+      out[b] = soff[b] | ((int64_t)col_bs[col[b]] << 56);
 }
 
 int32_t pack_plane_meta(Ctx* ctx, const DevMatrix* A, const MixedPlanes& mp, int64_t** a_meta) {
   LAMB_TRY(dalloc(ctx, a_meta, std::max<int64_t>(A->nnz, 1)));
   if (A->nnz) {
-    k_pack_plane_meta<<<grid_for(A->n_rows, 128), 128, 0, ctx->stream>>>(A->n_rows, A->row_p, A->col, A->col_bs,
+    k_pack_plane_meta<<<grid_for(32ll * A->n_rows, 256), 256, 0, ctx->stream>>>(A->n_rows, A->row_p, A->col, A->col_bs,
                                                                            mp.a_soff, *a_meta);
     LAMB_LAUNCHED(ctx);
   }

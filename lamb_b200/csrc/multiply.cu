@@ -391,8 +391,8 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
 __global__ void k_pack_offk(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                             const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                             const int8_t* __restrict__ col_bs, int k_is_col, int64_t* __restrict__ out) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b)
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps())
+    for (int64_t b = row_p[r] + (threadIdx.x & 31); b < row_p[r + 1]; b += 32)
       out[b] = off[b] | ((int64_t)(k_is_col ? col_bs[col[b]] : row_bs[r]) << 56);
 }
 
@@ -400,7 +400,7 @@ int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk) {
   LAMB_TRY(dalloc(ctx, offk, std::max<int64_t>(m->nnz, 1)));
   if (m->data_len > kOffMask) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "operand data too large");
   if (m->nnz) {
-    k_pack_offk<<<grid_for(m->n_rows, 128), 128, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->off, m->row_bs,
+    k_pack_offk<<<grid_for(32ll * m->n_rows, 256), 256, 0, ctx->stream>>>(m->n_rows, m->row_p, m->col, m->off, m->row_bs,
                                                                      m->col_bs, k_is_col ? 1 : 0, *offk);
     LAMB_LAUNCHED(ctx);
   }
@@ -413,15 +413,16 @@ __global__ void k_build_work(int32_t n_rows, const int32_t* __restrict__ order, 
                              const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                              const int8_t* __restrict__ col_bs, const int64_t* __restrict__ stack_p,
                              Work* __restrict__ work, int32_t* __restrict__ work_c) {
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n_rows; w += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t w = global_warp(); w < n_rows; w += grid_warps()) {
     const int r = order[w];
     const long long bi = row_bs[r];
-    int64_t v = cum[w];
-    for (int64_t c = row_p[r]; c < row_p[r + 1]; ++c, ++v) {
+    const int64_t c0 = row_p[r], v0 = cum[w] - c0;
+    for (int64_t c = c0 + lane; c < row_p[r + 1]; c += 32) {
       const long long bj = col_bs[col[c]];
       const long long n = stack_p[c + 1] - stack_p[c];
-      work[v] = Work{(long long)off[c] | (bi << 40) | (bj << 48), (long long)stack_p[c] | (n << 40)};
-      work_c[v] = (int32_t)c;
+      work[v0 + c] = Work{(long long)off[c] | (bi << 40) | (bj << 48), (long long)stack_p[c] | (n << 40)};
+      work_c[v0 + c] = (int32_t)c;
     }
   }
 }
@@ -455,7 +456,7 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
   k_order_lens<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, C->row_p, d_len);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, d_len, d_cum, n));
-  k_build_work<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, order_src->order, d_cum, C->row_p, C->col, C->off,
+  k_build_work<<<grid_for(32ll * n, 256), 256, 0, ctx->stream>>>(n, order_src->order, d_cum, C->row_p, C->col, C->off,
                                                             C->row_bs, C->col_bs, sym.stack_p, *work, *work_c);
   LAMB_LAUNCHED(ctx);
   dfree(ctx, d_len);
@@ -474,21 +475,23 @@ __global__ void k_keep_counts(int32_t n_rows, int32_t S, const int32_t* __restri
                               const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                               const double* __restrict__ c_nrm, double eps, int64_t* __restrict__ row_kept,
                               unsigned long long* __restrict__ sec_kept) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    int m = 0;
-    while (m + 1 < n_rsub && rsub_base[m + 1] <= r) ++m;
-    int n = 0;
-    int64_t k = 0, tot = 0;
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
-      while (col[b] >= csub_base[n + 1]) {
-        if (k) atomicAdd(&sec_kept[(int64_t)m * S + n], (unsigned long long)k);
-        tot += k; k = 0; ++n;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
+    const int m = row_subset(rsub_base, n_rsub, r);
+    const int64_t b1 = row_p[r + 1];
+    int64_t lo = row_p[r], tot = 0;
+    for (int n = 0; n < S; ++n) {
+      const int64_t hi = lower_col(col, lo, b1, csub_base[n + 1]);
+      int64_t k = 0;
+      for (int64_t b0 = lo; b0 < hi; b0 += 32) {
+        const int64_t b = b0 + lane;
+        k += __popc(__ballot_sync(0xffffffffu, b < hi && !(c_nrm[b] < eps)));
       }
-      k += !(c_nrm[b] < eps);
+      if (k && lane == 0) atomicAdd(&sec_kept[(int64_t)m * S + n], (unsigned long long)k);
+      tot += k;
+      lo = hi;
     }
-    if (k) atomicAdd(&sec_kept[(int64_t)m * S + n], (unsigned long long)k);
-    tot += k;
-    row_kept[r + 1] = tot;
+    if (lane == 0) row_kept[r + 1] = tot;
   }
 }
 
@@ -496,10 +499,22 @@ __global__ void k_compact(int32_t n_rows, const int64_t* __restrict__ row_p, con
                           const int64_t* __restrict__ off, const double* __restrict__ c_nrm, double eps,
                           const int64_t* __restrict__ new_row_p, int32_t* __restrict__ ncol,
                           int64_t* __restrict__ noff) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
     int64_t q = new_row_p[r];
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b)
-      if (!(c_nrm[b] < eps)) { ncol[q] = col[b]; noff[q] = off[b]; ++q; }
+    const int64_t b1 = row_p[r + 1];
+    for (int64_t b0 = row_p[r]; b0 < b1; b0 += 32) {
+      const int64_t b = b0 + lane;
+      const bool keep = b < b1 && !(c_nrm[b] < eps);
+      const unsigned kb = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int64_t p = q + __popc(kb & below);
+        ncol[p] = col[b];
+        noff[p] = off[b];
+      }
+      q += __popc(kb);
+    }
   }
 }
 
@@ -531,11 +546,11 @@ int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps) {
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_rb, C->rsub_base.data(), sizeof(int32_t) * (C->n_rsub + 1), cudaMemcpyHostToDevice, ctx->stream));
   LAMB_CUDA(ctx, cudaMemsetAsync(row_kept, 0, sizeof(int64_t), ctx->stream));
   LAMB_CUDA(ctx, cudaMemsetAsync(sec_kept, 0, sizeof(unsigned long long) * n_sec, ctx->stream));
-  k_keep_counts<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, S, d_cb, d_rb, C->n_rsub, C->row_p,
+  k_keep_counts<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, S, d_cb, d_rb, C->n_rsub, C->row_p,
                                                                     C->col, c_nrm, eps, row_kept, sec_kept);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(inclusive_scan_i64(ctx, row_kept, nrp, (int64_t)C->n_rows + 1));
-  k_compact<<<grid_for(C->n_rows, 128), 128, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, C->off, c_nrm, eps, nrp,
+  k_compact<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, C->off, c_nrm, eps, nrp,
                                                                 ncol, noff);
   LAMB_LAUNCHED(ctx);
   LAMB_CUDA(ctx, cudaMemcpyAsync(ctx->pend_h, sec_kept, sizeof(int64_t) * n_sec, cudaMemcpyDeviceToHost, ctx->stream));
