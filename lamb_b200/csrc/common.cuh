@@ -181,6 +181,8 @@ void free_sector_index(Ctx* ctx, SectorIndex* si);
 int32_t exclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int32_t inclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int32_t sum_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out);
+// Smallest of n doubles (waits for the stream); 0 when n == 0.
+int32_t min_f64(Ctx* ctx, const double* in, int64_t n, double* host_out);
 
 // ---- device helpers -------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {

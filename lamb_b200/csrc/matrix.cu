@@ -191,6 +191,24 @@ int32_t sum_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out) {
   return LAMB_GPU_OK;
 }
 
+int32_t min_f64(Ctx* ctx, const double* in, int64_t n, double* host_out) {
+  *host_out = 0.0;
+  if (n <= 0) return LAMB_GPU_OK;
+  double* d_out = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_out, 1));
+  size_t bytes = 0;
+  LAMB_CUDA(ctx, cub::DeviceReduce::Min(nullptr, bytes, in, d_out, n, ctx->stream));
+  void* tmp = nullptr;
+  LAMB_TRY(dalloc(ctx, (char**)&tmp, (int64_t)bytes + 16));
+  cudaError_t e = cub::DeviceReduce::Min(tmp, bytes, in, d_out, n, ctx->stream);
+  cudaFreeAsync(tmp, ctx->stream);
+  LAMB_CUDA(ctx, e);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_out);
+  return LAMB_GPU_OK;
+}
+
 // ---- block norms -----------------------------------------------------------------------
 // One warp per block row; each lane sums whole blocks sequentially (fixed order).
 __global__ void k_block_norms(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,

@@ -39,15 +39,22 @@ int32_t check_compatible(Ctx* ctx, const DevMatrix* A, const DevMatrix* B) {
 // reached by surviving products A_ik.B_kj (|A_ik|*|B_kj| >= eps).
 constexpr int kSymThreads = 256;
 
-__device__ __forceinline__ bool keep_pair(double na, double nb, double eps, int filt) {
-  return !(filt && na * nb < eps);
+// FILT = false when no product can fall below eps: the norms are then not read.
+template <bool FILT>
+__device__ __forceinline__ bool keep_pair(double na, const double* __restrict__ b_nrm, int64_t bb, double eps) {
+  return !FILT || !(na * b_nrm[bb] < eps);
 }
+// The fill always reads the norms (with eps = 0 when nothing is filtered:
+// norms are >= 0 or NaN, so every pair stays); its norm-free variant measured
+// 1.4 ms slower at 6,144 waters while the count kernel gains 0.8 ms.
+__device__ __forceinline__ bool keep_norms(double na, double nb, double eps) { return !(na * nb < eps); }
 
+template <bool FILT>
 __global__ void __launch_bounds__(kSymThreads) k_sym_count(
     int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
     const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
     const double* __restrict__ b_nrm, const int8_t* __restrict__ row_bs, const int8_t* __restrict__ k_bs,
-    const int8_t* __restrict__ col_bs, double eps, int filt, int32_t n_words, int64_t* __restrict__ c_cnt,
+    const int8_t* __restrict__ col_bs, double eps, int32_t n_words, int64_t* __restrict__ c_cnt,
     int64_t* __restrict__ s_cnt, int64_t* __restrict__ p_cnt, double* __restrict__ row_flops,
     unsigned* __restrict__ max_a_len) {
   extern __shared__ uint32_t bm[];
@@ -64,12 +71,12 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_count(
     const int bi = row_bs[i];
     for (int64_t ab = a_row_p[i] + warp; ab < a_row_p[i + 1]; ab += nw) {
       const int k = a_col[ab];
-      const double na = a_nrm[ab];
+      const double na = FILT ? a_nrm[ab] : 0.0;
       const int bk = k_bs[k];
       const int64_t b1 = b_row_p[k + 1];
       for (int64_t bb = b_row_p[k] + lane; bb < b1; bb += 32) {
         ++pairs;
-        if (!keep_pair(na, b_nrm[bb], eps, filt)) continue;
+        if (!keep_pair<FILT>(na, b_nrm, bb, eps)) continue;
         const int j = b_col[bb];
         atomicOr(&bm[j >> 5], 1u << (j & 31));
         ++kept;
@@ -139,7 +146,7 @@ template <bool IDS>
 __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
     const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
-    const double* __restrict__ b_nrm, double eps, int filt, int32_t n_words, int32_t na_max, int32_t nc_max,
+    const double* __restrict__ b_nrm, double eps, int32_t n_words, int32_t na_max, int32_t nc_max,
     const int64_t* __restrict__ c_row_p, const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col,
     int64_t* __restrict__ stack_p, const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off,
     Ent* __restrict__ ent, int2* __restrict__ ids) {
@@ -167,7 +174,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     for (int a = warp; a < na; a += nw) {
       const double x = s_anrm[a];
       for (int64_t bb = s_bbeg[a] + lane; bb < s_bend[a]; bb += 32)
-        if (keep_pair(x, b_nrm[bb], eps, filt)) {
+        if (keep_norms(x, b_nrm[bb], eps)) {
           const int j = b_col[bb];
           atomicOr(&bm[j >> 5], 1u << (j & 31));
         }
@@ -193,7 +200,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     for (int a = warp; a < na; a += nw) {
       const double x = s_anrm[a];
       for (int64_t bb = s_bbeg[a] + lane; bb < s_bend[a]; bb += 32)
-        if (keep_pair(x, b_nrm[bb], eps, filt)) atomicAdd(&cur[bm_rank(bm, wpre, b_col[bb])], 1);
+        if (keep_norms(x, b_nrm[bb], eps)) atomicAdd(&cur[bm_rank(bm, wpre, b_col[bb])], 1);
     }
     __syncthreads();
     block_excl_scan_smem(cur, nc);
@@ -220,7 +227,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
       const int njb = nhave ? b_col[nbb] : 0;
       const long long nob = (!IDS && nhave) ? b_off[nbb] : 0;
       while (have) {
-        if (keep_pair(x, nb, eps, filt)) {
+        if (keep_norms(x, nb, eps)) {
           const int p = bm_rank(bm, wpre, jb);
           const int slot = cur[p];
           cur[p] = slot + 1;
@@ -292,17 +299,28 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   unsigned* d_max_na = nullptr;
   LAMB_TRY(dalloc(ctx, &d_max_na, 1));
   LAMB_CUDA(ctx, cudaMemsetAsync(d_max_na, 0, sizeof(unsigned), ctx->stream));
-  const int fl = filt ? 1 : 0;
+  // No product falls below eps when the smallest norms of A and B multiply to
+  // at least eps (fl(x*y) is monotone in x and y): the count kernel then
+  // skips the norm loads.  Any NaN norm keeps the test.
+  bool count_filt = filt;
+  if (filt && A->nnz && B->nnz) {
+    double min_a = 0.0, min_b = 0.0;
+    LAMB_TRY(min_f64(ctx, A->norms, A->nnz, &min_a));
+    LAMB_TRY(min_f64(ctx, B->norms, B->nnz, &min_b));
+    if (min_a * min_b >= eps) count_filt = false;
+  }
+  const double fill_eps = filt ? eps : 0.0;
   const size_t smem_count = sizeof(uint32_t) * (size_t)std::max(n_words, 1);
   if (smem_count > 200 * 1024)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "too many block columns for the symbolic bitmap");
   if (n_rows > 0) {
+    auto count_kern = count_filt ? k_sym_count<true> : k_sym_count<false>;
     if (smem_count > 48 * 1024)
-      LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count));
+      LAMB_CUDA(ctx, cudaFuncSetAttribute(count_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count));
     int grid = 1;
-    LAMB_TRY(resident_grid(ctx, k_sym_count, smem_count, n_rows, &grid));
-    k_sym_count<<<grid, kSymThreads, smem_count, ctx->stream>>>(
-        n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, C->row_bs, B->row_bs, C->col_bs, eps, fl,
+    LAMB_TRY(resident_grid(ctx, count_kern, smem_count, n_rows, &grid));
+    count_kern<<<grid, kSymThreads, smem_count, ctx->stream>>>(
+        n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, C->row_bs, B->row_bs, C->col_bs, eps,
         n_words, c_cnt, s_cnt, p_cnt, rfl, d_max_na);
     LAMB_LAUNCHED(ctx);
   }
@@ -361,7 +379,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     int fgrid = 1;
     LAMB_TRY(resident_grid(ctx, kern, smem_fill, n_rows, &fgrid));
     kern<<<fgrid, kSymThreads, smem_fill, ctx->stream>>>(
-        n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, eps, fl, n_words, (int32_t)max_na,
+        n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, fill_eps, n_words, (int32_t)max_na,
         (int32_t)max_c, C->row_p, s_row_base, C->col, out->stack_p, a_offk, b_meta ? b_meta : B->off, out->ent,
         out->ids);
     LAMB_LAUNCHED(ctx);
