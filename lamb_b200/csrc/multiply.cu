@@ -246,7 +246,6 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
   }
 }
 
-// Shared memory of k_sym_fill for the given sizes.
 // Grid of a row-looping symbolic kernel: the CTAs that are resident at once
 // on all SMs (at most one per row).
 template <typename K>
@@ -258,6 +257,7 @@ static int32_t resident_grid(Ctx* ctx, K kern, size_t smem, int32_t n_rows, int*
   return LAMB_GPU_OK;
 }
 
+// Shared memory of k_sym_fill for the given sizes.
 static size_t sym_fill_smem(int32_t n_words, int64_t na_max, int64_t nc_max) {
   return (size_t)(32 * na_max + 8 * (int64_t)n_words + 4 * (nc_max + 1));
 }
