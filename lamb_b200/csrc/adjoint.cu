@@ -85,34 +85,47 @@ static int32_t transpose_index(Ctx* ctx, const DevMatrix* m, TIndex* t) {
 // For output block z = (r, c) of pattern Z: entries over the sorted
 // intersection of L's row r and R's row c (column lists lcol/rcol; block ids
 // lblk/rblk, or identity when null).  Entry = (L offset | inner << 56, R offset)
-// with inner = ksz[column].
+// with inner = ksz[column].  One warp per output block: lanes take 32 entries
+// of L's row at a time and binary-search their columns in R's row; a ballot
+// keeps the matches in ascending column order.
 template <bool FILL>
-__global__ void k_masked_sym(int32_t n_rows, const int64_t* __restrict__ zrp, const int32_t* __restrict__ zcol,
-                             const int64_t* __restrict__ lrp, const int32_t* __restrict__ lcol,
-                             const int32_t* __restrict__ lblk, const int64_t* __restrict__ loff,
-                             const int64_t* __restrict__ rrp, const int32_t* __restrict__ rcol,
-                             const int32_t* __restrict__ rblk, const int64_t* __restrict__ roff,
-                             const int8_t* __restrict__ ksz, int64_t* __restrict__ cnt,
-                             const int64_t* __restrict__ sp, Ent* __restrict__ ent) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    for (int64_t z = zrp[r]; z < zrp[r + 1]; ++z) {
-      const int c = zcol[z];
-      int64_t a = lrp[r], ae = lrp[r + 1], b = rrp[c], be = rrp[c + 1];
-      int64_t n = 0, w = FILL ? sp[z] : 0;
-      while (a < ae && b < be) {
-        const int ja = lcol[a], jb = rcol[b];
-        if (ja < jb) ++a;
-        else if (jb < ja) ++b;
-        else {
-          if (FILL) {
-            const int64_t la = lblk ? lblk[a] : a, rb = rblk ? rblk[b] : b;
-            ent[w++] = Ent{(long long)loff[la] | ((long long)ksz[ja] << 56), (long long)roff[rb]};
-          }
-          ++n; ++a; ++b;
-        }
-      }
-      if (!FILL) cnt[z] = n;
+__global__ void k_masked_sym(int32_t n_rows, int64_t n_z, const int64_t* __restrict__ zrp,
+                             const int32_t* __restrict__ zcol, const int64_t* __restrict__ lrp,
+                             const int32_t* __restrict__ lcol, const int32_t* __restrict__ lblk,
+                             const int64_t* __restrict__ loff, const int64_t* __restrict__ rrp,
+                             const int32_t* __restrict__ rcol, const int32_t* __restrict__ rblk,
+                             const int64_t* __restrict__ roff, const int8_t* __restrict__ ksz,
+                             int64_t* __restrict__ cnt, const int64_t* __restrict__ sp, Ent* __restrict__ ent) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  for (int64_t z = global_warp(); z < n_z; z += grid_warps()) {
+    int64_t lo = 0, hi = n_rows;  // the row r with zrp[r] <= z < zrp[r + 1]
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (zrp[mid] <= z) lo = mid; else hi = mid;
     }
+    const int64_t r = lo;
+    const int c = zcol[z];
+    const int64_t ae = lrp[r + 1], b0 = rrp[c], be = rrp[c + 1];
+    int64_t w = FILL ? sp[z] : 0, n = 0;
+    for (int64_t a = lrp[r]; a < ae; a += 32) {
+      const int64_t ai = a + lane;
+      int ja = 0;
+      int64_t bp = be;
+      if (ai < ae) {
+        ja = lcol[ai];
+        bp = lower_col(rcol, b0, be, ja);
+      }
+      const bool hit = bp < be && rcol[bp] == ja;
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (FILL && hit) {
+        const int64_t la = lblk ? lblk[ai] : ai, rb = rblk ? rblk[bp] : bp;
+        ent[w + __popc(m & below)] = Ent{(long long)loff[la] | ((long long)ksz[ja] << 56), (long long)roff[rb]};
+      }
+      w += __popc(m);
+      n += __popc(m);
+    }
+    if (!FILL && lane == 0) cnt[z] = n;
   }
 }
 
@@ -120,8 +133,8 @@ __global__ void k_masked_work(int32_t n_rows, const int64_t* __restrict__ zrp, c
                               const int64_t* __restrict__ zoff, const int8_t* __restrict__ rbs,
                               const int8_t* __restrict__ cbs, const int64_t* __restrict__ sp,
                               Work* __restrict__ work, int32_t* __restrict__ work_c) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x)
-    for (int64_t z = zrp[r]; z < zrp[r + 1]; ++z) {
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps())
+    for (int64_t z = zrp[r] + (threadIdx.x & 31); z < zrp[r + 1]; z += 32) {
       const long long M = rbs[r], N = cbs[zcol[z]], n = sp[z + 1] - sp[z];
       work[z] = Work{(long long)zoff[z] | (M << 40) | (N << 48), (long long)sp[z] | (n << 40)};
       work_c[z] = (int32_t)z;
@@ -156,8 +169,8 @@ static int32_t masked_product(Ctx* ctx, const DevMatrix* Z, DevMatrix* out, cons
   LAMB_TRY(dalloc(ctx, &cnt, out->nnz + 1));
   LAMB_TRY(dalloc(ctx, &sp, out->nnz + 1));
   LAMB_CUDA(ctx, cudaMemsetAsync(cnt + out->nnz, 0, sizeof(int64_t), ctx->stream));
-  k_masked_sym<false><<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, out->row_p, out->col, lrp, lcol, lblk, loff, rrp,
-                                                                   rcol, rblk, roff, ksz, cnt, nullptr, nullptr);
+  k_masked_sym<false><<<grid_for(32ll * out->nnz, 256), 256, 0, ctx->stream>>>(
+      n, out->nnz, out->row_p, out->col, lrp, lcol, lblk, loff, rrp, rcol, rblk, roff, ksz, cnt, nullptr, nullptr);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, cnt, sp, out->nnz + 1));
   int64_t n_ent = 0;
@@ -166,10 +179,10 @@ static int32_t masked_product(Ctx* ctx, const DevMatrix* Z, DevMatrix* out, cons
   LAMB_TRY(dalloc(ctx, &ent, std::max<int64_t>(n_ent, 1)));
   LAMB_TRY(dalloc(ctx, &work, out->nnz));
   LAMB_TRY(dalloc(ctx, &work_c, out->nnz));
-  k_masked_sym<true><<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, out->row_p, out->col, lrp, lcol, lblk, loff, rrp,
-                                                                  rcol, rblk, roff, ksz, nullptr, sp, ent);
+  k_masked_sym<true><<<grid_for(32ll * out->nnz, 256), 256, 0, ctx->stream>>>(
+      n, out->nnz, out->row_p, out->col, lrp, lcol, lblk, loff, rrp, rcol, rblk, roff, ksz, nullptr, sp, ent);
   LAMB_LAUNCHED(ctx);
-  k_masked_work<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, out->row_p, out->col, out->off, out->row_bs,
+  k_masked_work<<<grid_for(32ll * n, 256), 256, 0, ctx->stream>>>(n, out->row_p, out->col, out->off, out->row_bs,
                                                              out->col_bs, sp, work, work_c);
   LAMB_LAUNCHED(ctx);
   int32_t rc = run_stacked(ctx, out->nnz, work, work_c, ent, ldata, rdata, out->data, nullptr, t1, t2, max_inner);

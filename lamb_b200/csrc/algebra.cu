@@ -53,18 +53,29 @@ int32_t sum_f64(Ctx* ctx, const double* in, int64_t n, double* host_out) {
 }
 
 // ---- union pattern ----------------------------------------------------------------------
+// Union of the sorted block rows of X and Y, one warp per row.  The union
+// has |X| + |Y| - |X and Y| blocks.  The block at rank a of X's row sits at
+// union position a + (blocks of Y's row with a smaller column) - (columns in
+// both rows smaller than its own), the second term by binary search in Y's
+// row, the third by a running count of X's blocks found in Y; Y's blocks
+// likewise.  A column in both rows is written by the X side.
 __global__ void k_union_count(int32_t n_rows, const int64_t* __restrict__ xrp, const int32_t* __restrict__ xc,
                               const int64_t* __restrict__ yrp, const int32_t* __restrict__ yc,
                               int64_t* __restrict__ cnt) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = xrp[r], ae = xrp[r + 1], b = yrp[r], be = yrp[r + 1], n = 0;
-    while (a < ae || b < be) {
-      if (b >= be || (a < ae && xc[a] < yc[b])) ++a;
-      else if (a >= ae || yc[b] < xc[a]) ++b;
-      else { ++a; ++b; }
-      ++n;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
+    const int64_t a0 = xrp[r], ae = xrp[r + 1], b0 = yrp[r], be = yrp[r + 1];
+    int64_t both = 0;
+    for (int64_t a = a0; a < ae; a += 32) {
+      bool hit = false;
+      if (a + lane < ae) {
+        const int c = xc[a + lane];
+        const int64_t bp = lower_col(yc, b0, be, c);
+        hit = bp < be && yc[bp] == c;
+      }
+      both += __popc(__ballot_sync(0xffffffffu, hit));
     }
-    cnt[r] = n;
+    if (lane == 0) cnt[r] = (ae - a0) + (be - b0) - both;
   }
 }
 
@@ -72,13 +83,47 @@ __global__ void k_union_fill(int32_t n_rows, const int64_t* __restrict__ xrp, co
                              const int64_t* __restrict__ yrp, const int32_t* __restrict__ yc,
                              const int64_t* __restrict__ urp, int32_t* __restrict__ uc, int64_t* __restrict__ xi,
                              int64_t* __restrict__ yi) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = xrp[r], ae = xrp[r + 1], b = yrp[r], be = yrp[r + 1], u = urp[r];
-    while (a < ae || b < be) {
-      if (b >= be || (a < ae && xc[a] < yc[b])) { uc[u] = xc[a]; xi[u] = a; yi[u] = -1; ++a; }
-      else if (a >= ae || yc[b] < xc[a]) { uc[u] = yc[b]; xi[u] = -1; yi[u] = b; ++b; }
-      else { uc[u] = xc[a]; xi[u] = a; yi[u] = b; ++a; ++b; }
-      ++u;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
+    const int64_t a0 = xrp[r], ae = xrp[r + 1], b0 = yrp[r], be = yrp[r + 1], u0 = urp[r];
+    const unsigned below = (1u << lane) - 1u;
+    int64_t both = 0;  // columns in both rows before the current chunk of X
+    for (int64_t a1 = a0; a1 < ae; a1 += 32) {
+      const int64_t a = a1 + lane;
+      int c = 0;
+      int64_t bp = be;
+      if (a < ae) {
+        c = xc[a];
+        bp = lower_col(yc, b0, be, c);
+      }
+      const bool hit = bp < be && yc[bp] == c;
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (a < ae) {
+        const int64_t u = u0 + (a - a0) + (bp - b0) - (both + __popc(m & below));
+        uc[u] = c;
+        xi[u] = a;
+        yi[u] = hit ? bp : -1;
+      }
+      both += __popc(m);
+    }
+    both = 0;  // now: columns in both rows before the current chunk of Y
+    for (int64_t b1 = b0; b1 < be; b1 += 32) {
+      const int64_t b = b1 + lane;
+      int c = 0;
+      int64_t ap = ae;
+      if (b < be) {
+        c = yc[b];
+        ap = lower_col(xc, a0, ae, c);
+      }
+      const bool hit = ap < ae && xc[ap] == c;
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (b < be && !hit) {
+        const int64_t u = u0 + (b - b0) + (ap - a0) - (both + __popc(m & below));
+        uc[u] = c;
+        xi[u] = -1;
+        yi[u] = b;
+      }
+      both += __popc(m);
     }
   }
 }
@@ -94,7 +139,7 @@ int32_t union_pattern(Ctx* ctx, const DevMatrix* X, const DevMatrix* Y, DevMatri
   LAMB_TRY(dalloc(ctx, &cnt, std::max(n, 1)));
   LAMB_TRY(dalloc(ctx, &U->row_p, n + 1));
   if (n) {
-    k_union_count<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, X->row_p, X->col, Y->row_p, Y->col, cnt);
+    k_union_count<<<grid_for(32ll * n, 256), 256, 0, ctx->stream>>>(n, X->row_p, X->col, Y->row_p, Y->col, cnt);
     LAMB_LAUNCHED(ctx);
   }
   std::vector<int64_t> h(n), rp(n + 1, 0);
@@ -109,7 +154,7 @@ int32_t union_pattern(Ctx* ctx, const DevMatrix* X, const DevMatrix* Y, DevMatri
   LAMB_TRY(dalloc(ctx, xi, std::max<int64_t>(U->nnz, 1)));
   LAMB_TRY(dalloc(ctx, yi, std::max<int64_t>(U->nnz, 1)));
   if (U->nnz) {
-    k_union_fill<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, X->row_p, X->col, Y->row_p, Y->col, U->row_p, U->col,
+    k_union_fill<<<grid_for(32ll * n, 256), 256, 0, ctx->stream>>>(n, X->row_p, X->col, Y->row_p, Y->col, U->row_p, U->col,
                                                               *xi, *yi);
     LAMB_LAUNCHED(ctx);
   }
@@ -228,12 +273,11 @@ __global__ void k_scale(int64_t n, double* __restrict__ d, double alpha) {
 
 __global__ void k_identity(int32_t n_rows, const int64_t* __restrict__ row_p, const int64_t* __restrict__ off,
                            const int8_t* __restrict__ bs, double* __restrict__ d) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps()) {
     if (row_p[r + 1] == row_p[r]) continue;
     const int b = bs[r];
     double* p = d + off[row_p[r]];
-    for (int q = 0; q < b; ++q)
-      for (int e = 0; e < b; ++e) p[q * b + e] = (q == e) ? 1.0 : 0.0;
+    for (int e = threadIdx.x & 31; e < b * b; e += 32) p[e] = (e % b == e / b) ? 1.0 : 0.0;
   }
 }
 
@@ -257,7 +301,7 @@ int32_t identity_like(Ctx* ctx, const DevMatrix* X, DevMatrix* I) {
   LAMB_TRY(layout_sector_major(ctx, I, nullptr));
   LAMB_TRY(dalloc(ctx, &I->data, std::max<int64_t>(I->data_len, 1)));
   if (n) {
-    k_identity<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, I->row_p, I->off, I->row_bs, I->data);
+    k_identity<<<grid_for(32ll * n, 256), 256, 0, ctx->stream>>>(n, I->row_p, I->off, I->row_bs, I->data);
     LAMB_LAUNCHED(ctx);
   }
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
