@@ -3,8 +3,9 @@
  *
  * This header is the drop-in boundary between a single-rank LAMB run and the
  * GPU implementation of C = A . B over LAMB sector storage.  A Fortran caller
- * binds it with ISO_C_BINDING (interface blocks are given in INTEGRATION.md);
- * Python binds it with ctypes (lamb_b200/abi.py).
+ * binds it with ISO_C_BINDING (the interface module is
+ * lamb_b200/fortran/lamb_gpu_binding.F90); Python binds it with ctypes
+ * (lamb_b200/abi.py).
  *
  * Reference interfaces replaced (paths within uborstnik/LAMB):
  *   - lamb_multiply(matrix_a, matrix_b, matrix_c, error)
@@ -83,7 +84,8 @@ extern "C" {
 #define LAMB_GPU_NO_PRODUCT_FILTER 2u /* keep products with |A_ik||B_kj| < eps */
 #define LAMB_GPU_NO_RESULT_FILTER 4u  /* keep C blocks with |C_ij| < eps      */
 #define LAMB_GPU_ASYNC 8u             /* return once the work is queued (see lamb_gpu_multiply) */
-#define LAMB_GPU_ACCUMULATE 16u       /* C := C + A.B on C's existing blocks (pattern of C is extended) */
+#define LAMB_GPU_ACCUMULATE 16u       /* reserved: C := C + A.B; lamb_gpu_multiply refuses it with
+                                         lamb_unimplemented (accumulate with lamb_gpu_matrix_axpby) */
 
 /* One sector of a LAMB matrix in the reference's storage (see above). */
 typedef struct lamb_c_sector {
@@ -135,6 +137,9 @@ typedef struct lamb_gpu_mult_stats {
   double ms_total;           /* device time of the whole multiply             */
   int32_t mixed_slices;      /* int8 slices per operand (0 for FP64)          */
   int32_t kernel_launches;   /* this library's kernels launched by the call   */
+  double ms_prepare;         /* part of ms_symbolic spent preparing operands
+                                (mixed: digit planes / panels; FP64: 0)       */
+  double ms_filter;          /* device time of the result filter              */
 } lamb_gpu_mult_stats;
 
 typedef struct lamb_gpu_ctx lamb_gpu_ctx;
@@ -370,7 +375,11 @@ typedef struct lamb_gpu_dcsr {
  * storage in a fixed array inside the library: 8 MiB of device memory per
  * GPU, held from the library's first use on that GPU until the process
  * exits.  X may hold at most LAMB_GPU_NOALLOC_MAX_BLOCKS blocks; larger X is
- * rejected with a lamb_wrong_args status.  The first call on a device looks
+ * rejected with a lamb_wrong_args status, and so is a Y whose block Y_ji is
+ * not shaped like X_ij transposed (the two blockings differ).  An empty Y
+ * (nnz == 0) may pass null arrays; the trace is then 0.  A CUDA error that
+ * was already pending when the call starts is reported as
+ * lamb_external_error without launching anything.  The first call on a device looks
  * up that array's device address (cudaGetSymbolAddress) with the device
  * current; make that first call before any stream capture.  Every call uses
  * the same array, so calls whose work overlaps on the GPU (other streams or

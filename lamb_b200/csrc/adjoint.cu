@@ -173,9 +173,20 @@ static int32_t masked_product(Ctx* ctx, const DevMatrix* Z, DevMatrix* out, cons
       n, out->nnz, out->row_p, out->col, lrp, lcol, lblk, loff, rrp, rcol, rblk, roff, ksz, cnt, nullptr, nullptr);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, cnt, sp, out->nnz + 1));
-  int64_t n_ent = 0;
+  int64_t n_ent = 0, max_cnt = 0;
   LAMB_CUDA(ctx, cudaMemcpyAsync(&n_ent, sp + out->nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  LAMB_TRY(max_i64(ctx, cnt, out->nnz, &max_cnt));  // waits for the stream
+  // The work items pack the C data offset and the first entry in 40 bits and
+  // an entry count in 24 bits (as the forward multiply does).
+  auto release = [&]() { dfree(ctx, cnt); dfree(ctx, sp); };
+  if (n_ent >= (1ll << 40) || max_cnt >= (1ll << 24)) {
+    release();
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "adjoint: stack too large");
+  }
+  if (out->data_len >= kMask40) {
+    release();
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "adjoint: output data too large");
+  }
   LAMB_TRY(dalloc(ctx, &ent, std::max<int64_t>(n_ent, 1)));
   LAMB_TRY(dalloc(ctx, &work, out->nnz));
   LAMB_TRY(dalloc(ctx, &work_c, out->nnz));

@@ -206,6 +206,7 @@ void move_matrix(Ctx* ctx, DevMatrix* dst, DevMatrix* src) {
   free_matrix_buffers(ctx, dst);
   *dst = std::move(*src);
   *src = DevMatrix{};
+  touch(dst);
   if (!pos.empty() && dst->h_pos.empty() && (int64_t)pos.size() == 3ll * dst->n_rows) {
     dst->h_pos = pos;
     memcpy(dst->box, box, sizeof(box));

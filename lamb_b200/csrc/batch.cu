@@ -24,6 +24,11 @@ namespace lamb {
 struct Batch {
   Ctx* ctx = nullptr;
   std::vector<DevMatrix*> c;
+  // Every operand's handle and layout generation at creation: the graph holds
+  // their raw device pointers, so an execution is refused once any of them
+  // was destroyed, re-laid-out or reallocated.
+  std::vector<lamb_gpu_matrix> handles;
+  std::vector<uint64_t> gens;
   std::vector<Symbolic> sym;
   Work* work = nullptr;
   int32_t* work_c = nullptr;
@@ -198,7 +203,25 @@ static int32_t create_batch(Ctx* ctx, const lamb_gpu_matrix* a, const lamb_gpu_m
     dfree(ctx, B->sym[i].stack_p);
     dfree(ctx, B->sym[i].c_row);
   }
+  for (int i = 0; i < n; ++i)
+    for (lamb_gpu_matrix h : {a[i], b[i], c[i]}) {
+      B->handles.push_back(h);
+      B->gens.push_back(find_matrix(ctx, h)->gen);
+    }
   return autotune(B);
+}
+
+// The operands' buffers are those the graph was built on.
+static int32_t check_operands(Batch* B) {
+  Ctx* ctx = B->ctx;
+  for (size_t i = 0; i < B->handles.size(); ++i) {
+    const DevMatrix* m = find_matrix(ctx, B->handles[i]);
+    if (!m || m->gen != B->gens[i])
+      return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS,
+                  "batch: operand " + std::to_string(B->handles[i]) +
+                      " was destroyed or its buffers replaced since lamb_gpu_batch_create");
+  }
+  return LAMB_GPU_OK;
 }
 
 }  // namespace lamb
@@ -229,6 +252,8 @@ int32_t lamb_gpu_batch_execute(lamb_gpu_batch* bh, lamb_gpu_mult_stats* stats) {
   if (!B) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
   Ctx* ctx = B->ctx;
   cudaSetDevice(ctx->device);
+  LAMB_TRY(settle(ctx));
+  LAMB_TRY(check_operands(B));
   const int64_t launches0 = ctx->launches;
   if (!B->exec) {
     LAMB_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));

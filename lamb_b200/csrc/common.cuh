@@ -57,7 +57,14 @@ struct DevMatrix {
   int n_chunks = 0;
   std::vector<int64_t> chunk_rng;
   const double* chunk_data = nullptr;  // data buffer the ranges refer to
+  // Layout generation: a process-wide unique value renewed (touch()) whenever
+  // the device buffers or the block layout are replaced, so that holders of
+  // raw device pointers (batches) can detect a stale view.
+  uint64_t gen = 0;
 };
+
+// Gives m a new layout generation.
+void touch(DevMatrix* m);
 
 constexpr int kMaxChunks = 8;
 
@@ -181,6 +188,8 @@ void free_sector_index(Ctx* ctx, SectorIndex* si);
 int32_t exclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int32_t inclusive_scan_i64(Ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int32_t sum_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out);
+// Largest of n int64 (waits for the stream); 0 when n == 0.
+int32_t max_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out);
 // Smallest of n doubles (waits for the stream); 0 when n == 0.
 int32_t min_f64(Ctx* ctx, const double* in, int64_t n, double* host_out);
 

@@ -9,6 +9,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -98,7 +99,13 @@ DevMatrix* get_matrix(Ctx* ctx, lamb_gpu_matrix h) {
   return find_matrix(ctx, h);
 }
 
+void touch(DevMatrix* m) {
+  static std::atomic<uint64_t> g_gen{0};
+  m->gen = ++g_gen;
+}
+
 void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
+  touch(m);
   dfree(ctx, m->row_bs);
   dfree(ctx, m->col_bs);
   dfree(ctx, m->row_p);
@@ -117,6 +124,7 @@ void free_matrix_buffers(Ctx* ctx, DevMatrix* m) {
 
 int32_t register_matrix(Ctx* ctx, std::unique_ptr<DevMatrix> m, lamb_gpu_matrix* h) {
   *h = ctx->next_handle++;
+  touch(m.get());
   ctx->mats[*h] = std::move(m);
   return LAMB_GPU_OK;
 }
@@ -183,6 +191,24 @@ int32_t sum_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out) {
   void* tmp = nullptr;
   LAMB_TRY(dalloc(ctx, (char**)&tmp, (int64_t)bytes + 16));
   cudaError_t e = cub::DeviceReduce::Sum(tmp, bytes, in, d_out, n, ctx->stream);
+  cudaFreeAsync(tmp, ctx->stream);
+  LAMB_CUDA(ctx, e);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_out);
+  return LAMB_GPU_OK;
+}
+
+int32_t max_i64(Ctx* ctx, const int64_t* in, int64_t n, int64_t* host_out) {
+  *host_out = 0;
+  if (n <= 0) return LAMB_GPU_OK;
+  int64_t* d_out = nullptr;
+  LAMB_TRY(dalloc(ctx, &d_out, 1));
+  size_t bytes = 0;
+  LAMB_CUDA(ctx, cub::DeviceReduce::Max(nullptr, bytes, in, d_out, n, ctx->stream));
+  void* tmp = nullptr;
+  LAMB_TRY(dalloc(ctx, (char**)&tmp, (int64_t)bytes + 16));
+  cudaError_t e = cub::DeviceReduce::Max(tmp, bytes, in, d_out, n, ctx->stream);
   cudaFreeAsync(tmp, ctx->stream);
   LAMB_CUDA(ctx, e);
   LAMB_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));

@@ -404,7 +404,7 @@ static std::vector<int64_t> elem_base(const std::vector<int8_t>& bs) {
   return b;
 }
 
-int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp) {
+int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp, bool exps_only) {
   if (max_block(A->h_row_bs) > 127 || max_block(B->h_col_bs) > 127)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "mixed: block too large");
   static_assert(kThreads <= 256, "k_row_exp keeps 8 warps x 128 rows of maxima in shared memory");
@@ -429,6 +429,7 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
     LAMB_LAUNCHED(ctx);
   }
   trace_mark(ctx, "slice exponents");
+  if (exps_only) return LAMB_GPU_OK;
   // plane offsets
   int64_t* sz = nullptr;
   LAMB_TRY(dalloc(ctx, &mp->a_soff, std::max<int64_t>(A->nnz, 1) + 1));

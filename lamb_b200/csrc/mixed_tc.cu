@@ -1,0 +1,955 @@
+// Mixed-precision numeric phase on the 5th-generation tensor cores
+// (tcgen05.mma kind::i8, accumulators in tensor memory).  No reference
+// counterpart: the reference's sector_multiply (src/lamb_multiplication.F90:
+// 206-225) is a stub; this computes the same C = A.B as the FP64 path from
+// exact int8 digit products (the split-and-sum idea of Ozaki, Ogita, Oishi
+// and Rump, Numer. Algorithms 59 (2012), with fixed-point int8 digits).
+//
+// Digits.  Every element row r of A gets a power-of-two scale 2^ea_r >=
+// max_k |A(r,k)|, every element column c of B 2^eb_c >= max_k |B(k,c)|; a
+// scaled value x in (-1, 1) is written x = sum_p d_p / (127 * 254^p) + rest
+// with integer digits |d_p| <= 127 (t = 127 x; d_p = rint(t);
+// t = 254 (t - d_p)), i.e. almost 8 bits a digit: six digits carry 47 bits.
+// For S digits,
+//   C(r,c) = 2^(ea_r + eb_c) sum_{L=0}^{S-1} sum_{p+q=L} (D_p E_q)(r,c) / (127^2 254^L),
+// every D_p E_q is an exact int32 sum (S * 127^2 per inner index keeps
+// 22,190 inner indices exact for S = 6), and the recombination runs in FP64.
+// Pairs with p + q >= S are dropped (weight below 127^-2 254^-S).
+//
+// Tiles.  Block rows are too small for tcgen05 (M = 128), so the multiply is
+// done on spatial clusters: row atoms (in the row processing order, a Morton
+// curve over the atoms' coordinates) are cut into clusters of at most 128
+// rows, column atoms into clusters of at most 64 columns.  A cluster pair
+// (I, J) holding at least one C block is one tile; its inner dimension is the
+// concatenation of every inner atom k that couples to both clusters (some
+// A_ik with i in I and some B_kj with j in J), so only M and N are padded.
+// Operands live in "panels" built once per multiply: for row cluster I and
+// every inner atom k it touches, b_k panel rows of 128 bytes (the cluster's
+// rows, zero where A_ik is absent), one array per digit plane; B likewise
+// with 64-byte rows.  A K-row of a tile is thus one 128-byte A panel row and
+// one 64-byte B panel row, which the producer warps gather into shared memory
+// (cp.async, 16 bytes a thread) in the canonical MN-major layouts of UMMA
+// (128B swizzle for A, 64B swizzle for B).  Products that the product filter
+// would skip are included (they are bounded by eps each); the C pattern is
+// the filtered one, so only C blocks of the pattern are written.
+//
+// Kernel roles (one CTA of 256 threads per SM, persistent over the tiles):
+//   warps 0-2  producers: gather the tile's K rows, 32 per pipeline stage
+//              (two warps the A chunks, one warp the B chunks);
+//   warp 3     loads each tile's inner-atom list one tile ahead, allocates
+//              the tensor memory (6 levels x 64 columns in 512) and from one
+//              lane issues S(S+1)/2 MMAs (M=128, N=64, K=32) per stage;
+//   warps 4-7  epilogue: tensor memory -> registers, FP64 recombination,
+//              scaling, scatter into C's blocks and their norms.
+// Every wait on an mbarrier is bounded (2 s of %globaltimer); on a timeout
+// the kernel records an error code, every role stops, and the host returns
+// an error status.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <numeric>
+
+#include "multiply.cuh"
+
+namespace lamb {
+namespace tc {
+
+constexpr int kS = 6;                 // digits per operand
+constexpr int kM = 128, kN = 64, kK = 32;
+constexpr int kStages = 4;
+constexpr int kPlaneA = kK * kM;      // bytes of one digit plane of one stage (A)
+constexpr int kPlaneB = kK * kN;
+constexpr int kStageA = kS * kPlaneA;
+constexpr int kStageB = kS * kPlaneB;
+constexpr int kStageBytes = kStageA + kStageB;  // 36,864: a multiple of 1,024
+constexpr int kMaxEnt = 1024;         // inner atoms of one tile
+constexpr int kMaxRowAtoms = 32;      // atoms of one row cluster
+constexpr int kMaxColAtoms = 16;      // atoms of one column cluster
+constexpr int kTileThreads = 256;
+constexpr int kProducers = 96;
+constexpr int kTmemCols = 512;
+constexpr int64_t kRowMask = (1 << 25) - 1;  // panel row of an entry (bk in the top 7 bits)
+// Level accumulators stay exact while (K rows) * S * 127^2 < 2^31.
+constexpr int64_t kMaxKRows = (int64_t)INT_MAX / (kS * 127 * 127);
+constexpr double kFirst = 127.0, kBase = 254.0;
+// Weight of level L: 1 / (127^2 254^L).
+__device__ constexpr double kLevelW[kS] = {1.0 / 16129.0, 1.0 / (16129.0 * 254.0), 1.0 / (16129.0 * 64516.0),
+                                          1.0 / (16129.0 * 16387064.0), 1.0 / (16129.0 * 4162314256.0),
+                                          1.0 / (16129.0 * 1057227821024.0)};
+
+enum : int { kErrTimeoutFull = 1, kErrTimeoutEmpty = 2, kErrTimeoutTmemFull = 4, kErrTimeoutTmemEmpty = 8,
+             kErrTimeoutEnt = 16, kErrTimeoutDone = 32, kErrEntries = 64 };
+
+// ---- shared-memory layout of the tile kernel --------------------------------------------
+struct __align__(16) TileSmem {
+  // entries of two tiles (the loader fills one while the producers use the other)
+  int32_t ent_a[2][kMaxEnt];
+  int32_t ent_b[2][kMaxEnt];
+  int32_t ent_pre[2][kMaxEnt + 1];
+  int32_t ent_n[2];
+  // epilogue tables of the current tile
+  int32_t blk[kMaxRowAtoms * kMaxColAtoms];
+  long long off[kMaxRowAtoms * kMaxColAtoms];
+  double part[kM][kMaxColAtoms];
+  int16_t row_atom[kM];   // atom index within the row cluster, -1 for padding rows
+  int8_t row_pe[kM];
+  int32_t row_exp[kM];
+  int8_t row_b[kMaxRowAtoms];
+  int16_t row_off[kMaxRowAtoms];
+  int16_t col_atom[kN];
+  int8_t col_q[kN];
+  int8_t col_last[kN];
+  int32_t col_exp[kN];
+  int32_t n_ra, n_ca;
+  unsigned long long bar_full[kStages], bar_empty[kStages];
+  unsigned long long bar_tmem_full, bar_tmem_empty, bar_ent_full[2], bar_ent_empty[2], bar_done;
+  uint32_t tmem_base;
+  int abort;
+};
+
+constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + sizeof(TileSmem) + 1024;  // + alignment slack
+
+struct TcArgs {
+  const int2* tiles;
+  int64_t n_tiles;
+  const int64_t* ent_base;
+  const int64_t* ent_cnt;
+  const int32_t* krows;
+  const uint2* ent;
+  const int8_t* pan_a;
+  int64_t plane_a;  // bytes between digit planes of the A panels
+  const int8_t* pan_b;
+  int64_t plane_b;
+  const int32_t* rc_first;
+  const int32_t* rc_atoms;
+  const int32_t* cc_first;
+  const int32_t* cc_atoms;
+  const int8_t* row_bs;  // C (= A) row block sizes
+  const int8_t* col_bs;  // C (= B) column block sizes
+  const int64_t* rbase;  // first element row of every A row atom
+  const int64_t* cbase;  // first element column of every B column atom
+  const int* ea;
+  const int* eb;
+  const int32_t* tblk;   // [tile][kMaxRowAtoms][kMaxColAtoms] C block id or -1
+  const int64_t* c_off;
+  double* c_data;
+  double* c_nrm;
+  int* err;
+};
+
+// ---- PTX helpers -----------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void bar_init(unsigned long long* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(unsigned long long* b) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool bar_try(unsigned long long* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits until the phase with the given parity has completed; gives up after
+// 2 s (or when another role aborted), recording `code`.
+__device__ __forceinline__ bool bar_wait(unsigned long long* b, uint32_t parity, TileSmem* sm, int* err, int code) {
+  if (bar_try(b, parity)) return true;
+  const uint64_t t0 = now_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (bar_try(b, parity)) return true;
+    if ((it & 255) == 0) {
+      if (*(volatile int*)&sm->abort) return false;
+      if (now_ns() - t0 > 2000000000ull) {
+        atomicOr(err, code);
+        *(volatile int*)&sm->abort = 1;
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+// Arrive on the mbarrier once every cp.async this thread issued so far has
+// landed (counts as one of the barrier's expected arrivals).
+__device__ __forceinline__ void cp_arrive(unsigned long long* b) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor (tcgen05): start address, leading / stride
+// byte offsets (16-byte units), version 1, swizzle mode.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t swizzle) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3fff);
+  d |= (uint64_t)((lbo >> 4) & 0x3fff) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3fff) << 32;
+  d |= (uint64_t)1 << 46;              // descriptor version (Blackwell)
+  d |= (uint64_t)(swizzle & 7) << 61;  // 2: 128-byte swizzle, 4: 64-byte swizzle
+  return d;
+}
+// Instruction descriptor: kind::i8, signed A and B, int32 accumulator, both
+// operands MN-major, N = 64, M = 128.
+constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(unsigned long long* b) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Byte offset of (inner row kk, 16-byte chunk c) of one digit plane of a
+// stage: A rows are 128 bytes, 128-byte swizzle (chunk ^= row % 8); B rows
+// are 64 bytes, 64-byte swizzle (chunk ^= (row / 2) % 4).
+__device__ __forceinline__ uint32_t a_swz(int kk, int c) { return (uint32_t)(kk * 128 + ((c ^ (kk & 7)) << 4)); }
+__device__ __forceinline__ uint32_t b_swz(int kk, int c) { return (uint32_t)(kk * 64 + ((c ^ ((kk >> 1) & 3)) << 4)); }
+
+// ---- the tile kernel ------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* stages = base;
+  TileSmem* sm = reinterpret_cast<TileSmem*>(base + (size_t)kStages * kStageBytes);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      bar_init(&sm->bar_full[s], kProducers);
+      bar_init(&sm->bar_empty[s], 1);
+    }
+    bar_init(&sm->bar_tmem_full, 1);
+    bar_init(&sm->bar_tmem_empty, 128);
+    for (int b = 0; b < 2; ++b) {
+      bar_init(&sm->bar_ent_full[b], 32);
+      bar_init(&sm->bar_ent_empty[b], kProducers);
+    }
+    bar_init(&sm->bar_done, 1);
+    sm->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 3) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm->tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm->tmem_base;
+  const int64_t n_tiles = g.n_tiles;
+
+  if (warp < 3) {
+    // ================= producers =================
+    const int pt = tid;  // 0..95
+    const int kr = pt & 31, grp = pt >> 5;
+    int64_t gs = 0;      // stages issued by this CTA so far
+    int64_t local = 0;
+    for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
+      const int buf = (int)(local & 1);
+      if (!bar_wait(&sm->bar_ent_full[buf], (uint32_t)((local >> 1) & 1), sm, g.err, kErrTimeoutEnt)) break;
+      const int n = sm->ent_n[buf];
+      const int K = g.krows[t];
+      const int nst = K > 0 ? (K + kK - 1) / kK : 1;
+      const int32_t* pre = sm->ent_pre[buf];
+      for (int s = 0; s < nst; ++s, ++gs) {
+        const int stg = (int)(gs % kStages);
+        if (!bar_wait(&sm->bar_empty[stg], (uint32_t)(((gs / kStages) & 1) ^ 1), sm, g.err, kErrTimeoutEmpty)) break;
+        const int kk = s * kK + kr;
+        const bool valid = kk < K;
+        int64_t arow = 0, brow = 0;
+        if (valid) {
+          int lo = 0, hi = n - 1;  // last entry e with pre[e] <= kk
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= kk) lo = mid; else hi = mid - 1;
+          }
+          arow = sm->ent_a[buf][lo] + (kk - pre[lo]);
+          brow = sm->ent_b[buf][lo] + (kk - pre[lo]);
+        }
+        const uint32_t sa = smem_u32(stages + (size_t)stg * kStageBytes);
+        const uint32_t sb = sa + kStageA;
+        const uint32_t bytes = valid ? 16u : 0u;
+        if (grp < 2) {  // A chunks 4 grp .. 4 grp + 3 of the row
+#pragma unroll
+          for (int p = 0; p < kS; ++p) {
+            const int8_t* src = g.pan_a + p * g.plane_a + arow * 128;
+#pragma unroll
+            for (int c = 4 * grp; c < 4 * grp + 4; ++c) cp16(sa + p * kPlaneA + a_swz(kr, c), src + 16 * c, bytes);
+          }
+        } else {        // the row's 4 B chunks
+#pragma unroll
+          for (int p = 0; p < kS; ++p) {
+            const int8_t* src = g.pan_b + p * g.plane_b + brow * 64;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) cp16(sb + p * kPlaneB + b_swz(kr, c), src + 16 * c, bytes);
+          }
+        }
+        cp_arrive(&sm->bar_full[stg]);
+      }
+      // the entry buffer of this tile may be refilled once every producer is past it
+      bar_arrive(&sm->bar_ent_empty[buf]);
+    }
+  } else if (warp >= 4) {
+    // ================= epilogue =================
+    const int et = tid - 128;       // 0..127: tile row m
+    const int ew = warp - 4;        // tensor-memory lane quarter
+    int64_t local = 0;
+    for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
+      const int I = g.tiles[t].x, J = g.tiles[t].y;
+      const int r0 = g.rc_first[I], nra = g.rc_first[I + 1] - r0;
+      const int c0 = g.cc_first[J], nca = g.cc_first[J + 1] - c0;
+      // ---- tables of this tile (the MMAs of the tile run meanwhile) ----
+      if (et < kM) { sm->row_atom[et] = -1; sm->row_pe[et] = 0; sm->row_exp[et] = 0; }
+      if (et < kN) { sm->col_atom[et] = -1; sm->col_q[et] = 0; sm->col_last[et] = 0; sm->col_exp[et] = 0; }
+      if (et == 0) {
+        int o = 0;
+        for (int a = 0; a < nra; ++a) {
+          const int b = g.row_bs[g.rc_atoms[r0 + a]];
+          sm->row_b[a] = (int8_t)b;
+          sm->row_off[a] = (int16_t)o;
+          o += b;
+        }
+        sm->n_ra = nra;
+        sm->n_ca = nca;
+      }
+      named_sync(2, 128);
+      for (int a = et >> 5; a < nra; a += 4) {  // rows of atom a
+        const int atom = g.rc_atoms[r0 + a], b = sm->row_b[a], o = sm->row_off[a];
+        for (int pe = lane; pe < b; pe += 32) {
+          sm->row_atom[o + pe] = (int16_t)a;
+          sm->row_pe[o + pe] = (int8_t)pe;
+          sm->row_exp[o + pe] = g.ea[g.rbase[atom] + pe];
+        }
+      }
+      if (et < 32) {
+        int o = 0;
+        for (int b = 0; b < nca; ++b) {
+          const int atom = g.cc_atoms[c0 + b], w = g.col_bs[atom];
+          for (int q = lane; q < w; q += 32) {
+            sm->col_atom[o + q] = (int16_t)b;
+            sm->col_q[o + q] = (int8_t)q;
+            sm->col_last[o + q] = q == w - 1;
+            sm->col_exp[o + q] = g.eb[g.cbase[atom] + q];
+          }
+          o += w;
+        }
+      }
+      for (int p = et; p < nra * kMaxColAtoms; p += 128) {
+        const int a = p / kMaxColAtoms, b = p % kMaxColAtoms;
+        const int32_t bid = b < nca ? g.tblk[t * (kMaxRowAtoms * kMaxColAtoms) + a * kMaxColAtoms + b] : -1;
+        sm->blk[p] = bid;
+        sm->off[p] = bid >= 0 ? g.c_off[bid] : -1;
+      }
+      named_sync(2, 128);
+      // ---- accumulators ----
+      if (!bar_wait(&sm->bar_tmem_full, (uint32_t)(local & 1), sm, g.err, kErrTimeoutTmemFull)) break;
+      tc_fence_after();
+      double acc[kN];
+#pragma unroll
+      for (int n = 0; n < kN; ++n) acc[n] = 0.0;
+#pragma unroll
+      for (int L = kS - 1; L >= 0; --L) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int v[32];
+          tmem_ld32(tmem + ((uint32_t)(32 * ew) << 16) + (uint32_t)(64 * L + 32 * h), v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 32; ++c) acc[32 * h + c] = __fma_rn((double)v[c], kLevelW[L], acc[32 * h + c]);
+        }
+      }
+      tc_fence_before();
+      bar_arrive(&sm->bar_tmem_empty);
+      // ---- scaling and scatter ----
+      const int a = sm->row_atom[et];
+      double run = 0.0;
+      if (a >= 0) {
+        const int pe = sm->row_pe[et], bi = sm->row_b[a], er = sm->row_exp[et];
+#pragma unroll
+        for (int n = 0; n < kN; ++n) {
+          const int b = sm->col_atom[n];
+          if (b >= 0) {
+            const long long o = sm->off[a * kMaxColAtoms + b];
+            if (o >= 0) {
+              const double val = ldexp(acc[n], er + sm->col_exp[n]);
+              g.c_data[o + (int64_t)sm->col_q[n] * bi + pe] = val;
+              run = __fma_rn(val, val, run);
+            }
+            if (sm->col_last[n]) {
+              sm->part[et][b] = run;
+              run = 0.0;
+            }
+          }
+        }
+      }
+      named_sync(2, 128);
+      // ---- block norms in a fixed order (rows of the block ascending) ----
+      for (int p = et; p < nra * kMaxColAtoms; p += 128) {
+        const int32_t bid = sm->blk[p];
+        if (bid < 0) continue;
+        const int aa = p / kMaxColAtoms, b = p % kMaxColAtoms;
+        double s = 0.0;
+        for (int pe = 0; pe < sm->row_b[aa]; ++pe) s += sm->part[sm->row_off[aa] + pe][b];
+        g.c_nrm[bid] = __dsqrt_rn(s);
+      }
+      named_sync(2, 128);
+    }
+  } else {
+    // ================= warp 3: entry loader (all lanes) and MMA issuer (lane 0) =================
+    // The loader runs one tile ahead of the producers: entries of tile
+    // `local` go to buffer local % 2.  The MMA issuer follows the stages.
+    // Both live in this warp; the loader work for tile local+1 is done
+    // between the MMA batches of tile local (entries are small).
+    int64_t gs = 0, local_mma = 0;
+    int64_t load_next = blockIdx.x, load_local = 0;
+    auto load_entries = [&](int64_t t, int64_t lidx) -> bool {
+      const int buf = (int)(lidx & 1);
+      if (!bar_wait(&sm->bar_ent_empty[buf], (uint32_t)(((lidx >> 1) & 1) ^ 1), sm, g.err, kErrTimeoutEnt))
+        return false;
+      const int n = (int)g.ent_cnt[t];
+      const int64_t eb = g.ent_base[t];
+      if (n > kMaxEnt) { atomicOr(g.err, kErrEntries); sm->abort = 1; return false; }
+      int carry = 0;
+      for (int e0 = 0; e0 < n; e0 += 32) {
+        const int e = e0 + lane;
+        uint2 x = make_uint2(0u, 0u);
+        if (e < n) x = g.ent[eb + e];
+        const int bk = (int)(x.x >> 25);
+        int incl = bk;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        if (e < n) {
+          sm->ent_a[buf][e] = (int32_t)(x.x & kRowMask);
+          sm->ent_b[buf][e] = (int32_t)x.y;
+          sm->ent_pre[buf][e] = carry + incl - bk;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (lane == 0) {
+        sm->ent_pre[buf][n] = carry;
+        sm->ent_n[buf] = n;
+      }
+      __syncwarp();
+      bar_arrive(&sm->bar_ent_full[buf]);
+      return true;
+    };
+    bool ok = true;
+    // first tile's entries before any MMA
+    if (load_next < n_tiles) {
+      ok = load_entries(load_next, load_local);
+      load_next += gridDim.x;
+      ++load_local;
+    }
+    for (int64_t t = blockIdx.x; ok && t < n_tiles && !sm->abort; t += gridDim.x, ++local_mma) {
+      // the next tile's entries (the producers are on this tile now)
+      if (load_next < n_tiles) {
+        ok = load_entries(load_next, load_local);
+        load_next += gridDim.x;
+        ++load_local;
+        if (!ok) break;
+      }
+      const int K = g.krows[t];
+      const int nst = K > 0 ? (K + kK - 1) / kK : 1;
+      // tensor memory is free once the epilogue has read the previous tile
+      if (!bar_wait(&sm->bar_tmem_empty, (uint32_t)((local_mma & 1) ^ 1), sm, g.err, kErrTimeoutTmemEmpty)) break;
+      tc_fence_after();
+      for (int s = 0; s < nst; ++s, ++gs) {
+        const int stg = (int)(gs % kStages);
+        if (!bar_wait(&sm->bar_full[stg], (uint32_t)((gs / kStages) & 1), sm, g.err, kErrTimeoutFull)) { ok = false; break; }
+        tc_fence_after();
+        if (lane == 0) {
+          fence_async_smem();
+          const uint32_t sa = smem_u32(stages + (size_t)stg * kStageBytes);
+          const uint32_t sb = sa + kStageA;
+#pragma unroll
+          for (int L = 0; L < kS; ++L)
+#pragma unroll
+            for (int p = 0; p <= L; ++p) {
+              const int q = L - p;
+              const uint64_t da = smem_desc(sa + p * kPlaneA, 128, 1024, 2);
+              const uint64_t db = smem_desc(sb + q * kPlaneB, 64, 512, 4);
+              mma_i8(tmem + (uint32_t)(64 * L), da, db, (s > 0 || p > 0) ? 1u : 0u);
+            }
+          mma_commit(&sm->bar_empty[stg]);
+        }
+        __syncwarp();
+      }
+      if (!ok) break;
+      if (lane == 0) mma_commit(&sm->bar_tmem_full);
+      __syncwarp();
+    }
+    // every MMA issued by this CTA has completed before tensor memory is released
+    if (lane == 0) mma_commit(&sm->bar_done);
+    __syncwarp();
+    bar_wait(&sm->bar_done, 0, sm, g.err, kErrTimeoutDone);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 3)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+}  // namespace tc
+}  // namespace lamb
+
+// ============================================================================================
+// Preparation: clusters, inner-atom bitmaps, digit panels, tiles and their inner lists.
+// ============================================================================================
+namespace lamb {
+namespace tc {
+
+// Bitmap bit (cluster, inner atom k): A (by_row): cluster of row r, k = column;
+// B (!by_row): cluster of column c, k = row r.
+__global__ void k_tc_bitmap(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                            const int32_t* __restrict__ clus, int by_row, int32_t W, uint32_t* __restrict__ bm) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = global_warp(); r < n_rows; r += grid_warps())
+    for (int64_t b = row_p[r] + lane; b < row_p[r + 1]; b += 32) {
+      const int c = col[b];
+      const int cl = by_row ? clus[r] : clus[c];
+      const int k = by_row ? c : (int)r;
+      atomicOr(&bm[(int64_t)cl * W + (k >> 5)], 1u << (k & 31));
+    }
+}
+
+// Per cluster and bitmap word: inner atoms and panel rows (sum of their block
+// sizes) before the word; per cluster the totals.  One warp per cluster.
+__global__ void k_tc_word_prefix(int32_t n_cl, int32_t W, const uint32_t* __restrict__ bm,
+                                 const int8_t* __restrict__ kbs, int32_t* __restrict__ wrow,
+                                 int64_t* __restrict__ tot_row) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t c = global_warp(); c < n_cl; c += grid_warps()) {
+    int carry = 0;
+    for (int w0 = 0; w0 < W; w0 += 32) {
+      const int w = w0 + lane;
+      uint32_t bits = w < W ? bm[c * W + w] : 0u;
+      int rows = 0;
+      while (bits) {
+        const int bit = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        rows += kbs[32 * w + bit];
+      }
+      const int incl = warp_incl_scan(rows, lane);
+      if (w < W) wrow[c * W + w] = carry + incl - rows;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) tot_row[c] = carry;
+  }
+}
+
+// Panel row of inner atom k within cluster c's panel (relative to its base).
+__device__ __forceinline__ int64_t panel_row(const uint32_t* __restrict__ bm, const int32_t* __restrict__ wrow,
+                                             const int8_t* __restrict__ kbs, int64_t c, int32_t W, int k) {
+  const int w = k >> 5;
+  uint32_t below = bm[c * W + w] & ((1u << (k & 31)) - 1u);
+  int64_t r = wrow[c * W + w];
+  while (below) {
+    const int bit = __ffs(below) - 1;
+    below &= below - 1u;
+    r += kbs[32 * w + bit];
+  }
+  return r;
+}
+
+// Writes the S digits of x (|x| < 1) to S planes: |127 x| < 127 and every
+// later t lies in [-127, 127], so each digit fits int8.
+__device__ __forceinline__ void put_digits(int8_t* __restrict__ pan, int64_t plane, int64_t pos, double x) {
+  double t = x * kFirst;
+#pragma unroll
+  for (int p = 0; p < kS; ++p) {
+    const double dg = rint(t);
+    pan[p * plane + pos] = (int8_t)dg;
+    t = (t - dg) * kBase;
+  }
+}
+
+// A panels: element (pe, kc) of block (i, k) goes to panel row
+// base[I] + row(I, k) + kc, byte roff[i] + pe of that 128-byte row.
+__global__ void k_tc_digits_a(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                              const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                              const int8_t* __restrict__ kbs, const double* __restrict__ data,
+                              const int32_t* __restrict__ rcl, const int32_t* __restrict__ roff, int32_t W,
+                              const uint32_t* __restrict__ bm, const int32_t* __restrict__ wrow,
+                              const int64_t* __restrict__ base, const int64_t* __restrict__ rbase,
+                              const int* __restrict__ ea, int64_t plane, int8_t* __restrict__ pan) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = global_warp(); i < n_rows; i += grid_warps()) {
+    const int I = rcl[i], m0 = roff[i], bi = row_bs[i];
+    const int64_t e0 = rbase[i];
+    for (int64_t b = row_p[i]; b < row_p[i + 1]; ++b) {
+      const int k = col[b], bk = kbs[k];
+      int64_t prow = 0;
+      if (lane == 0) prow = base[I] + panel_row(bm, wrow, kbs, I, W, k);
+      prow = __shfl_sync(0xffffffffu, prow, 0);
+      const double* x = data + off[b];
+      for (int e = lane; e < bi * bk; e += 32) {
+        const int pe = e % bi, kc = e / bi;
+        put_digits(pan, plane, (prow + kc) * 128 + m0 + pe, ldexp(x[e], -ea[e0 + pe]));
+      }
+    }
+  }
+}
+
+// B panels: element (kr, q) of block (k, j) goes to panel row
+// base[J] + row(J, k) + kr, byte coff[j] + q of that 64-byte row.
+__global__ void k_tc_digits_b(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                              const int64_t* __restrict__ off, const int8_t* __restrict__ kbs,
+                              const int8_t* __restrict__ col_bs, const double* __restrict__ data,
+                              const int32_t* __restrict__ ccl, const int32_t* __restrict__ coff, int32_t W,
+                              const uint32_t* __restrict__ bm, const int32_t* __restrict__ wrow,
+                              const int64_t* __restrict__ base, const int64_t* __restrict__ cbase,
+                              const int* __restrict__ eb, int64_t plane, int8_t* __restrict__ pan) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t k = global_warp(); k < n_rows; k += grid_warps()) {
+    const int bk = kbs[k];
+    for (int64_t b = row_p[k]; b < row_p[k + 1]; ++b) {
+      const int j = col[b], J = ccl[j], n0 = coff[j], bj = col_bs[j];
+      int64_t prow = 0;
+      if (lane == 0) prow = base[J] + panel_row(bm, wrow, kbs, J, W, (int)k);
+      prow = __shfl_sync(0xffffffffu, prow, 0);
+      const double* x = data + off[b];
+      const int64_t e0 = cbase[j];
+      for (int e = lane; e < bk * bj; e += 32) {
+        const int kr = e % bk, q = e / bk;
+        put_digits(pan, plane, (prow + kr) * 64 + n0 + q, ldexp(x[e], -eb[e0 + q]));
+      }
+    }
+  }
+}
+
+// Tile flags: (row cluster, column cluster) pairs holding a C block.
+__global__ void k_tc_tile_flags(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                                const int32_t* __restrict__ rcl, const int32_t* __restrict__ ccl, int32_t n_cc,
+                                int64_t* __restrict__ flag) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = global_warp(); i < n_rows; i += grid_warps()) {
+    const int64_t I = rcl[i];
+    for (int64_t b = row_p[i] + lane; b < row_p[i + 1]; b += 32) flag[I * n_cc + ccl[col[b]]] = 1;
+  }
+}
+
+__global__ void k_tc_tile_list(int64_t n_map, int32_t n_cc, const int64_t* __restrict__ flag,
+                               const int64_t* __restrict__ pos, int2* __restrict__ tiles) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n_map; x += (int64_t)gridDim.x * blockDim.x)
+    if (flag[x]) tiles[pos[x]] = make_int2((int)(x / n_cc), (int)(x % n_cc));
+}
+
+// C block ids of every tile, at [tile][row atom][column atom].
+__global__ void k_tc_tile_blocks(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
+                                 const int32_t* __restrict__ rcl, const int32_t* __restrict__ ratom,
+                                 const int32_t* __restrict__ ccl, const int32_t* __restrict__ catom, int32_t n_cc,
+                                 const int64_t* __restrict__ pos, int32_t* __restrict__ tblk) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = global_warp(); i < n_rows; i += grid_warps()) {
+    const int64_t I = rcl[i];
+    const int a = ratom[i];
+    for (int64_t b = row_p[i] + lane; b < row_p[i + 1]; b += 32) {
+      const int j = col[b];
+      const int64_t t = pos[I * n_cc + ccl[j]];
+      tblk[t * (kMaxRowAtoms * kMaxColAtoms) + a * kMaxColAtoms + catom[j]] = (int32_t)b;
+    }
+  }
+}
+
+// Inner atoms of every tile: k with A_ik for some i in I and B_kj for some j
+// in J (and b_k > 0).  Count pass: entries and panel rows per tile.  Fill
+// pass: (A panel row | b_k << 25, B panel row) per entry.  One warp per tile.
+template <bool FILL>
+__global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int32_t W,
+                            const uint32_t* __restrict__ bma, const uint32_t* __restrict__ bmb,
+                            const int32_t* __restrict__ wra, const int32_t* __restrict__ wrb,
+                            const int64_t* __restrict__ basea, const int64_t* __restrict__ baseb,
+                            const int8_t* __restrict__ kbs, int64_t* __restrict__ cnt, int32_t* __restrict__ rows,
+                            const int64_t* __restrict__ ebase, uint2* __restrict__ ent) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t t = global_warp(); t < n_tiles; t += grid_warps()) {
+    const int64_t I = tiles[t].x, J = tiles[t].y;
+    int64_t carry = FILL ? ebase[t] : 0;
+    int nrows = 0;
+    for (int w0 = 0; w0 < W; w0 += 32) {
+      const int w = w0 + lane;
+      const uint32_t xa = w < W ? bma[I * W + w] : 0u, xb = w < W ? bmb[J * W + w] : 0u;
+      uint32_t x = xa & xb;
+      int c = 0;
+      for (uint32_t y = x; y;) {
+        const int bit = __ffs(y) - 1;
+        y &= y - 1u;
+        const int bk = kbs[32 * w + bit];
+        if (bk > 0) { ++c; nrows += bk; }
+      }
+      if (FILL) {
+        const int incl = warp_incl_scan(c, lane);
+        int64_t p = carry + incl - c;
+        while (x) {
+          const int bit = __ffs(x) - 1;
+          x &= x - 1u;
+          const int k = 32 * w + bit, bk = kbs[k];
+          if (bk == 0) continue;
+          const int64_t ar = basea[I] + panel_row(bma, wra, kbs, I, W, k);
+          const int64_t br = baseb[J] + panel_row(bmb, wrb, kbs, J, W, k);
+          ent[p++] = make_uint2((uint32_t)ar | ((uint32_t)bk << 25), (uint32_t)br);
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      } else {
+        carry += warp_sum_ll(c);
+      }
+    }
+    if (!FILL) {
+      nrows = (int)warp_sum_ll(nrows);
+      if (lane == 0) {
+        cnt[t] = carry;
+        rows[t] = nrows;
+      }
+    }
+  }
+}
+
+// ---- host ----------------------------------------------------------------------------------
+struct Clusters {
+  int32_t n = 0;
+  std::vector<int32_t> of, idx, off, first, atoms;
+};
+
+// Greedy cut of `order` into clusters of at most max_rows rows and max_atoms atoms.
+static Clusters make_clusters(const std::vector<int32_t>& order, const std::vector<int8_t>& bs, int max_rows,
+                              int max_atoms) {
+  Clusters c;
+  const size_t n = bs.size();
+  c.of.assign(n, 0);
+  c.idx.assign(n, 0);
+  c.off.assign(n, 0);
+  int rows = 0, atoms = 0;
+  for (size_t t = 0; t < order.size(); ++t) {
+    const int a = order[t], b = bs[a];
+    if (c.first.empty() || rows + b > max_rows || atoms == max_atoms) {
+      c.first.push_back((int32_t)c.atoms.size());
+      rows = 0;
+      atoms = 0;
+    }
+    c.of[a] = (int32_t)c.first.size() - 1;
+    c.idx[a] = atoms;
+    c.off[a] = rows;
+    c.atoms.push_back(a);
+    rows += b;
+    ++atoms;
+  }
+  c.n = (int32_t)c.first.size();
+  c.first.push_back((int32_t)c.atoms.size());
+  return c;
+}
+
+template <typename T>
+static int32_t upload_vec(Ctx* ctx, const std::vector<T>& v, T** d) {
+  LAMB_TRY(dalloc(ctx, d, std::max<int64_t>((int64_t)v.size(), 1)));
+  if (!v.empty()) LAMB_CUDA(ctx, cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
+  return LAMB_GPU_OK;
+}
+
+// Device buffers of one call, released (stream-ordered) when it returns.
+struct Bufs {
+  Ctx* ctx;
+  std::vector<void*> p;
+  ~Bufs() {
+    for (void* x : p)
+      if (x) cudaFreeAsync(x, ctx->stream);
+  }
+  template <typename T>
+  int32_t alloc(T** d, int64_t n) {
+    LAMB_TRY(dalloc(ctx, d, std::max<int64_t>(n, 1)));
+    p.push_back(*d);
+    return LAMB_GPU_OK;
+  }
+  template <typename T>
+  int32_t up(const std::vector<T>& v, T** d) {
+    LAMB_TRY(upload_vec(ctx, v, d));
+    p.push_back(*d);
+    return LAMB_GPU_OK;
+  }
+};
+
+}  // namespace tc
+
+bool mixed_tc_eligible(const DevMatrix* A, const DevMatrix* B) {
+  return max_block(A->h_row_bs) <= tc::kM && max_block(B->h_col_bs) <= tc::kN && A->n_rows > 0 && B->n_cols > 0 &&
+         A->nnz > 0 && B->nnz > 0;
+}
+
+// Numeric phase of a mixed multiply on tcgen05 (C's pattern, layout and data
+// buffer already set by a pattern-only symbolic phase).  Sets *ran = false,
+// leaving C untouched, when a tile exceeds the kernel's limits (inner atoms
+// or rows); the caller then uses the mma.sync path.
+int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const MixedPlanes& mp, double* c_nrm,
+                         bool* ran, cudaEvent_t ev_prepared) {
+  using namespace tc;
+  *ran = false;
+  if (C->nnz == 0) { *ran = true; return LAMB_GPU_OK; }
+  // ---- clusters (host, from the row processing order) ----
+  if ((int)A->h_order.size() != A->n_rows) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "mixed: row order missing");
+  const Clusters rc = make_clusters(A->h_order, A->h_row_bs, kM, kMaxRowAtoms);
+  std::vector<int32_t> corder(B->n_cols);
+  if (B->n_cols == A->n_rows && B->h_col_bs == A->h_row_bs)
+    corder = A->h_order;
+  else
+    std::iota(corder.begin(), corder.end(), 0);
+  const Clusters cc = make_clusters(corder, B->h_col_bs, kN, kMaxColAtoms);
+  const int32_t nk = A->n_cols, W = (nk + 31) / 32;
+  Bufs m{ctx, {}};
+  int32_t *d_rcl, *d_ratom, *d_roff, *d_rcf, *d_rca, *d_ccl, *d_catom, *d_coff, *d_ccf, *d_cca;
+  LAMB_TRY(m.up(rc.of, &d_rcl)); LAMB_TRY(m.up(rc.idx, &d_ratom)); LAMB_TRY(m.up(rc.off, &d_roff));
+  LAMB_TRY(m.up(rc.first, &d_rcf)); LAMB_TRY(m.up(rc.atoms, &d_rca));
+  LAMB_TRY(m.up(cc.of, &d_ccl)); LAMB_TRY(m.up(cc.idx, &d_catom)); LAMB_TRY(m.up(cc.off, &d_coff));
+  LAMB_TRY(m.up(cc.first, &d_ccf)); LAMB_TRY(m.up(cc.atoms, &d_cca));
+  // ---- inner-atom bitmaps and panel row offsets ----
+  uint32_t *bma, *bmb;
+  int32_t *wra, *wrb;
+  int64_t *tra, *trb, *basea, *baseb;
+  LAMB_TRY(m.alloc(&bma, (int64_t)rc.n * W)); LAMB_TRY(m.alloc(&bmb, (int64_t)cc.n * W));
+  LAMB_TRY(m.alloc(&wra, (int64_t)rc.n * W)); LAMB_TRY(m.alloc(&wrb, (int64_t)cc.n * W));
+  LAMB_TRY(m.alloc(&tra, rc.n + 1)); LAMB_TRY(m.alloc(&trb, cc.n + 1));
+  LAMB_TRY(m.alloc(&basea, rc.n + 1)); LAMB_TRY(m.alloc(&baseb, cc.n + 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(bma, 0, sizeof(uint32_t) * (size_t)rc.n * W, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemsetAsync(bmb, 0, sizeof(uint32_t) * (size_t)cc.n * W, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemsetAsync(tra + rc.n, 0, sizeof(int64_t), ctx->stream));
+  LAMB_CUDA(ctx, cudaMemsetAsync(trb + cc.n, 0, sizeof(int64_t), ctx->stream));
+  k_tc_bitmap<<<grid_for(32ll * A->n_rows, 256), 256, 0, ctx->stream>>>(A->n_rows, A->row_p, A->col, d_rcl, 1, W, bma);
+  LAMB_LAUNCHED(ctx);
+  k_tc_bitmap<<<grid_for(32ll * B->n_rows, 256), 256, 0, ctx->stream>>>(B->n_rows, B->row_p, B->col, d_ccl, 0, W, bmb);
+  LAMB_LAUNCHED(ctx);
+  k_tc_word_prefix<<<grid_for(32ll * rc.n, 256), 256, 0, ctx->stream>>>(rc.n, W, bma, A->col_bs, wra, tra);
+  LAMB_LAUNCHED(ctx);
+  k_tc_word_prefix<<<grid_for(32ll * cc.n, 256), 256, 0, ctx->stream>>>(cc.n, W, bmb, B->row_bs, wrb, trb);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, tra, basea, rc.n + 1));
+  LAMB_TRY(exclusive_scan_i64(ctx, trb, baseb, cc.n + 1));
+  int64_t ra = 0, rb = 0;
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&ra, basea + rc.n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&rb, baseb + cc.n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ra + 1 > kRowMask || rb + 1 > INT_MAX) return LAMB_GPU_OK;  // panel rows beyond the entry format: not run
+  // ---- digit panels (one zero row at the end of each plane for padding reads) ----
+  const int64_t plane_a = ((ra + 1) * 128 + 255) & ~255ll, plane_b = ((rb + 1) * 64 + 255) & ~255ll;
+  int8_t *pan_a = nullptr, *pan_b = nullptr;
+  LAMB_TRY(scratch(ctx, kScrPlaneA, plane_a * kS, &pan_a));
+  LAMB_TRY(scratch(ctx, kScrPlaneB, plane_b * kS, &pan_b));
+  LAMB_CUDA(ctx, cudaMemsetAsync(pan_a, 0, (size_t)(plane_a * kS), ctx->stream));
+  LAMB_CUDA(ctx, cudaMemsetAsync(pan_b, 0, (size_t)(plane_b * kS), ctx->stream));
+  k_tc_digits_a<<<grid_for(32ll * A->n_rows, 256), 256, 0, ctx->stream>>>(
+      A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, d_rcl, d_roff, W, bma, wra, basea, mp.rbase,
+      mp.ea, plane_a, pan_a);
+  LAMB_LAUNCHED(ctx);
+  k_tc_digits_b<<<grid_for(32ll * B->n_rows, 256), 256, 0, ctx->stream>>>(
+      B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, d_ccl, d_coff, W, bmb, wrb, baseb, mp.cbase,
+      mp.eb, plane_b, pan_b);
+  LAMB_LAUNCHED(ctx);
+  // ---- tiles ----
+  const int64_t n_map = (int64_t)rc.n * cc.n;
+  int64_t *flag, *pos;
+  LAMB_TRY(m.alloc(&flag, n_map + 1)); LAMB_TRY(m.alloc(&pos, n_map + 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int64_t) * (size_t)(n_map + 1), ctx->stream));
+  k_tc_tile_flags<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, d_rcl, d_ccl,
+                                                                         cc.n, flag);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, flag, pos, n_map + 1));
+  int64_t n_tiles = 0;
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&n_tiles, pos + n_map, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int2* tiles;
+  int32_t *tblk, *krows;
+  int64_t *ecnt, *ebase;
+  LAMB_TRY(m.alloc(&tiles, n_tiles));
+  LAMB_TRY(m.alloc(&tblk, n_tiles * (kMaxRowAtoms * kMaxColAtoms)));
+  LAMB_TRY(m.alloc(&krows, n_tiles));
+  LAMB_TRY(m.alloc(&ecnt, n_tiles + 1));
+  LAMB_TRY(m.alloc(&ebase, n_tiles + 1));
+  k_tc_tile_list<<<grid_for(n_map, 256), 256, 0, ctx->stream>>>(n_map, cc.n, flag, pos, tiles);
+  LAMB_LAUNCHED(ctx);
+  LAMB_CUDA(ctx, cudaMemsetAsync(tblk, 0xff, sizeof(int32_t) * (size_t)n_tiles * kMaxRowAtoms * kMaxColAtoms, ctx->stream));
+  k_tc_tile_blocks<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, d_rcl, d_ratom,
+                                                                          d_ccl, d_catom, cc.n, pos, tblk);
+  LAMB_LAUNCHED(ctx);
+  LAMB_CUDA(ctx, cudaMemsetAsync(ecnt + n_tiles, 0, sizeof(int64_t), ctx->stream));
+  k_tc_tile_k<false><<<grid_for(32ll * n_tiles, 256), 256, 0, ctx->stream>>>(
+      n_tiles, tiles, W, bma, bmb, wra, wrb, basea, baseb, A->col_bs, ecnt, krows, nullptr, nullptr);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, ecnt, ebase, n_tiles + 1));
+  int64_t n_ent = 0, max_ent = 0, max_rows = 0;
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&n_ent, ebase + n_tiles, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_TRY(max_i64(ctx, ecnt, n_tiles, &max_ent));
+  {
+    std::vector<int32_t> h(n_tiles);
+    LAMB_CUDA(ctx, cudaMemcpyAsync(h.data(), krows, sizeof(int32_t) * (size_t)n_tiles, cudaMemcpyDeviceToHost, ctx->stream));
+    LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int32_t x : h) max_rows = std::max<int64_t>(max_rows, x);
+  }
+  if (max_ent > kMaxEnt || max_rows > kMaxKRows) return LAMB_GPU_OK;  // outside the kernel's limits: not run
+  uint2* ent;
+  LAMB_TRY(m.alloc(&ent, n_ent));
+  k_tc_tile_k<true><<<grid_for(32ll * n_tiles, 256), 256, 0, ctx->stream>>>(
+      n_tiles, tiles, W, bma, bmb, wra, wrb, basea, baseb, A->col_bs, nullptr, nullptr, ebase, ent);
+  LAMB_LAUNCHED(ctx);
+  if (ev_prepared) LAMB_CUDA(ctx, cudaEventRecord(ev_prepared, ctx->stream));
+  // ---- the tile kernel ----
+  int* d_err;
+  LAMB_TRY(m.alloc(&d_err, 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  TcArgs g{};
+  g.tiles = tiles; g.n_tiles = n_tiles; g.ent_base = ebase; g.ent_cnt = ecnt; g.krows = krows; g.ent = ent;
+  g.pan_a = pan_a; g.plane_a = plane_a; g.pan_b = pan_b; g.plane_b = plane_b;
+  g.rc_first = d_rcf; g.rc_atoms = d_rca; g.cc_first = d_ccf; g.cc_atoms = d_cca;
+  g.row_bs = C->row_bs; g.col_bs = C->col_bs; g.rbase = mp.rbase; g.cbase = mp.cbase; g.ea = mp.ea; g.eb = mp.eb;
+  g.tblk = tblk; g.c_off = C->off; g.c_data = C->data; g.c_nrm = c_nrm; g.err = d_err;
+  LAMB_CUDA(ctx, cudaFuncSetAttribute(k_tc_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int grid = (int)std::min<int64_t>(n_tiles, sms);
+  k_tc_tiles<<<grid, kTileThreads, kSmemBytes, ctx->stream>>>(g);
+  LAMB_LAUNCHED(ctx);
+  int h_err = 0;
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h_err)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR,
+                "mixed: tensor-core tile kernel stopped (code " + std::to_string(h_err) + ")");
+  *ran = true;
+  return LAMB_GPU_OK;
+}
+
+}  // namespace lamb

@@ -11,6 +11,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <numeric>
 
 #include "multiply.cuh"
@@ -129,6 +130,48 @@ __device__ int block_excl_scan_smem(int* v, int n) {
 
 __device__ __forceinline__ int bm_rank(const uint32_t* bm, const int* wpre, int j) {
   return wpre[j >> 5] + __popc(bm[j >> 5] & ((1u << (j & 31)) - 1u));
+}
+
+// C pattern only (no stacks), one CTA per C row: the bitmap of reached
+// columns, then the row's columns in ascending order.  Used by the mixed
+// tensor-core path, which needs no block-product stacks.
+__global__ void __launch_bounds__(kSymThreads) k_sym_pattern(
+    int32_t n_rows, const int64_t* __restrict__ a_row_p, const int32_t* __restrict__ a_col,
+    const double* __restrict__ a_nrm, const int64_t* __restrict__ b_row_p, const int32_t* __restrict__ b_col,
+    const double* __restrict__ b_nrm, double eps, int32_t n_words, const int64_t* __restrict__ c_row_p,
+    int32_t* __restrict__ c_col) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);
+  int* wpre = reinterpret_cast<int*>(bm + n_words);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kSymThreads / 32;
+  for (int64_t i = blockIdx.x; i < n_rows; i += gridDim.x) {
+    for (int w = tid; w < n_words; w += kSymThreads) bm[w] = 0u;
+    __syncthreads();
+    for (int64_t ab = a_row_p[i] + warp; ab < a_row_p[i + 1]; ab += nw) {
+      const int k = a_col[ab];
+      const double x = a_nrm[ab];
+      for (int64_t bb = b_row_p[k] + lane; bb < b_row_p[k + 1]; bb += 32)
+        if (keep_norms(x, b_nrm[bb], eps)) {
+          const int j = b_col[bb];
+          atomicOr(&bm[j >> 5], 1u << (j & 31));
+        }
+    }
+    __syncthreads();
+    for (int w = tid; w < n_words; w += kSymThreads) wpre[w] = __popc(bm[w]);
+    __syncthreads();
+    block_excl_scan_smem(wpre, n_words);
+    const int64_t c0 = c_row_p[i];
+    for (int w = tid; w < n_words; w += kSymThreads) {
+      uint32_t bits = bm[w];
+      int p = wpre[w];
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        c_col[c0 + p++] = w * 32 + b;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Stack fill, one CTA per C row.  The row's A blocks (column norm, operand
@@ -272,7 +315,8 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   trace_mark(ctx, "operand norms");
   if (A->nnz >= (1ll << 31) || B->nnz >= (1ll << 31))
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "more than 2^31 blocks in an operand");
-  if (!want_ids && !a_offk) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "symbolic: no A meta");
+  if (!want_ids && !a_offk && !out->pattern_only)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "symbolic: no A meta");
   // C takes A's row subsets and B's column subsets.  Its data buffer is kept
   // for the new pattern when large enough (freed on every early return).
   struct KeptData {
@@ -360,6 +404,8 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_TRY(dalloc(ctx, &out->stack_p, C->nnz + 1));
   if (want_ids)
     LAMB_TRY(dalloc(ctx, &out->ids, std::max<int64_t>(out->n_ent, 1)));
+  else if (out->pattern_only)
+    out->ent = nullptr;
   else if (out->use_scratch)
     LAMB_TRY(scratch(ctx, kScrEnt, out->n_ent, &out->ent));
   else
@@ -367,9 +413,19 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
   trace_mark(ctx, "symbolic allocations");
   const size_t smem_fill = sym_fill_smem(std::max(n_words, 1), std::max<int64_t>(max_na, 1), max_c);
-  if (smem_fill > 220 * 1024)
+  if (out->pattern_only && n_rows > 0 && C->nnz > 0) {
+    const size_t smem_pat = sizeof(uint32_t) * 2 * (size_t)std::max(n_words, 1);
+    if (smem_pat > 48 * 1024)
+      LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pat));
+    int pgrid = 1;
+    LAMB_TRY(resident_grid(ctx, k_sym_pattern, smem_pat, n_rows, &pgrid));
+    k_sym_pattern<<<pgrid, kSymThreads, smem_pat, ctx->stream>>>(n_rows, A->row_p, A->col, A->norms, B->row_p, B->col,
+                                                                B->norms, fill_eps, n_words, C->row_p, C->col);
+    LAMB_LAUNCHED(ctx);
+  } else if (smem_fill > 220 * 1024) {
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
-  if (n_rows > 0 && C->nnz > 0) {
+  }
+  if (!out->pattern_only && n_rows > 0 && C->nnz > 0) {
     auto kern = want_ids ? k_sym_fill<true> : k_sym_fill<false>;
     if (smem_fill > 48 * 1024)
       LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
@@ -575,6 +631,7 @@ int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps) {
   LAMB_CUDA(ctx, cudaEventRecord(ctx->pend_ev, ctx->stream));
   dfree(ctx, C->row_p); dfree(ctx, C->col); dfree(ctx, C->off);
   C->row_p = nrp; C->col = ncol; C->off = noff;
+  touch(C);
   C->norms_valid = false;
   dfree(ctx, row_kept); dfree(ctx, sec_kept); dfree(ctx, d_cb); dfree(ctx, d_rb);
   ctx->pend_m = C;
@@ -693,6 +750,9 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   int64_t dropped = 0;
   MixedPlanes mp;
   const bool mixed = (flags & LAMB_GPU_MIXED) != 0;
+  // LAMB_GPU_MIXED_MMA_SYNC=1 selects the mma.sync digit kernel for every shape.
+  const char* force_sync = std::getenv("LAMB_GPU_MIXED_MMA_SYNC");
+  bool tc_path = mixed && mixed_tc_eligible(A, B) && !(force_sync && force_sync[0] == '1');
   sym.use_scratch = true;
   LAMB_TRY(settle(ctx));
   auto body = [&]() -> int32_t {
@@ -700,9 +760,40 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
     LAMB_TRY(check_compatible(ctx, A, B));
     LAMB_TRY(ensure_row_order(ctx, A));
     trace_mark(ctx, "row order");
+    if (mixed && tc_path) {
+      // tensor-core path: exponents, C's pattern (no stacks), then panels,
+      // tiles and the tile kernel inside numeric_mixed_tc
+      slices = kMixedTcSlices;
+      LAMB_TRY(build_slices(ctx, A, B, slices, &mp, true));
+      sym.pattern_only = true;
+      LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, nullptr, &sym));
+      LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
+      if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
+      trace_mark(ctx, "symbolic (pattern)");
+      bool ran = false;
+      LAMB_TRY(numeric_mixed_tc(ctx, A, B, C, mp, c_nrm, &ran, timed ? ctx->ev[1] : nullptr));
+      trace_mark(ctx, "numeric (tensor cores)");
+      if (ran) {
+        if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+        if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps));
+        trace_mark(ctx, "result filter");
+        if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+        return LAMB_GPU_OK;
+      }
+      // a tile beyond the kernel's limits: the mma.sync path below
+      tc_path = false;
+      free_slices(ctx, &mp);
+      mp = MixedPlanes{};
+      dfree(ctx, c_nrm);
+      free_symbolic(ctx, sym);
+      sym = Symbolic{};
+      sym.use_scratch = true;
+      if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    }
     if (mixed) {
       slices = mixed_slices_from_env();
       LAMB_TRY(build_slices(ctx, A, B, slices, &mp));
+      if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
       trace_mark(ctx, "digit slices");
       LAMB_TRY(pack_plane_meta(ctx, A, mp, &a_offk));
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym, mp.b_soff));
@@ -749,13 +840,20 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   st.kernel_launches = (int32_t)(ctx->launches - launches0);
   if (timed) {
     LAMB_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
-    float t01 = 0, t12 = 0, t03 = 0;
+    float t01 = 0, t12 = 0, t03 = 0, t23 = 0, t04 = 0;
     cudaEventElapsedTime(&t01, ctx->ev[0], ctx->ev[1]);
     cudaEventElapsedTime(&t12, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&t03, ctx->ev[0], ctx->ev[3]);
+    cudaEventElapsedTime(&t23, ctx->ev[2], ctx->ev[3]);
+    if (mixed && tc_path)
+      cudaEventElapsedTime(&t04, ctx->ev[4], ctx->ev[1]);  // panels, tiles and inner lists
+    else if (mixed)
+      cudaEventElapsedTime(&t04, ctx->ev[0], ctx->ev[4]);  // digit planes
     st.ms_symbolic = t01;
     st.ms_numeric = t12;
     st.ms_total = t03;
+    st.ms_filter = t23;
+    st.ms_prepare = t04;
   }
   ctx->last_stats = st;
   if (stats) *stats = st;

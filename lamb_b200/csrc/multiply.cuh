@@ -40,6 +40,7 @@ struct Symbolic {
   std::vector<int64_t> h_row_len;  // C blocks per row (host)
   std::vector<int64_t> h_base;     // C data offset of every (row subset, column subset, rank) run
   bool use_scratch = false;    // set before symbolic_phase: ent lives in the context's scratch
+  bool pattern_only = false;   // set before symbolic_phase: C's pattern and layout only, no stacks
 };
 void free_symbolic(Ctx* ctx, Symbolic& s);
 
@@ -91,7 +92,14 @@ struct MixedPlanes {
   int8_t *a_planes = nullptr, *b_planes = nullptr;
 };
 int mixed_slices_from_env();
-int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp);
+// exps_only: only the row / column exponents (and element bases), no planes.
+int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp, bool exps_only = false);
+// Mixed path on tcgen05 (mixed_tc.cu): shape limits, and the numeric phase
+// on cluster tiles (C's pattern set by a pattern-only symbolic phase).
+bool mixed_tc_eligible(const DevMatrix* A, const DevMatrix* B);
+constexpr int kMixedTcSlices = 6;
+int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const MixedPlanes& mp, double* c_nrm,
+                         bool* ran, cudaEvent_t ev_prepared);
 void free_slices(Ctx* ctx, MixedPlanes* mp);
 int32_t pack_plane_meta(Ctx* ctx, const DevMatrix* A, const MixedPlanes& mp, int64_t** a_meta);
 int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,

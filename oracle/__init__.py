@@ -20,6 +20,7 @@ from lamb_b200.matrix import LambMatrix
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liblamb_oracle.so")
 LONG_DOUBLE = 0x100
+NO_STACKS = 0x200
 NO_PRODUCT_FILTER = 2
 NO_RESULT_FILTER = 4
 
@@ -45,6 +46,9 @@ def lib():
                                         C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.lamb_oracle_stacks.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]
         L.lamb_oracle_free.argtypes = [C.c_void_p]
+        L.lamb_oracle_compare.argtypes = [C.c_void_p, C.POINTER(CSector), C.c_int32, C.c_double, C.c_int32,
+                                          C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
         L.lamb_oracle_block_norm.argtypes = [C.c_void_p, C.c_int64]
         L.lamb_oracle_block_norm.restype = C.c_double
         _lib = L
@@ -85,6 +89,35 @@ def multiply(a: LambMatrix, b: LambMatrix, eps: float = 0.0, flags: int = 0, thr
             L.lamb_oracle_stacks(h, ent.ctypes.data, C.byref(n))
             out.append(ent[:n.value])
         return tuple(out)
+    finally:
+        L.lamb_oracle_free(h)
+
+
+def check_product(a: LambMatrix, b: LambMatrix, eps: float, got: LambMatrix, flags: int = 0,
+                  threads: int = 0) -> dict:
+    """Whole-product check of a device result `got` (computed with the result
+    filter at eps) without copying the oracle's C into Python: the oracle
+    computes C = A.B without the result filter, then counts pattern
+    mismatches under the filter rule and the relative Frobenius error over the
+    kept blocks (lamb_oracle_compare)."""
+    L = lib()
+    ca, cb, cg = _arr(a), _arr(b), _arr(got)
+    h = C.c_void_p()
+    rc = L.lamb_oracle_multiply(ca, len(a.sectors), cb, len(b.sectors), eps, flags | NO_RESULT_FILTER | NO_STACKS,
+                                threads, 1, C.byref(h))
+    if rc != 0:
+        raise RuntimeError(f"oracle multiply failed ({rc})")
+    try:
+        mis, num, den, gap = C.c_int64(), C.c_double(), C.c_double(), C.c_double()
+        if L.lamb_oracle_compare(h, cg, len(got.sectors), eps, threads, C.byref(mis), C.byref(num), C.byref(den),
+                                 C.byref(gap)) != 0:
+            raise RuntimeError("oracle compare failed")
+        npr, nsk, ndr = C.c_int64(), C.c_int64(), C.c_int64()
+        fl = C.c_double()
+        L.lamb_oracle_stats(h, C.byref(npr), C.byref(nsk), C.byref(fl), C.byref(ndr))
+        rel = float(np.sqrt(num.value / den.value)) if den.value > 0 else float(np.sqrt(num.value))
+        return {"pattern_mismatches": mis.value, "rel_frobenius_err": rel, "min_rel_gap_to_eps": gap.value,
+                "n_products": npr.value, "n_products_skipped": nsk.value, "flops": fl.value}
     finally:
         L.lamb_oracle_free(h)
 

@@ -100,7 +100,7 @@ int32_t lamb_oracle_multiply(const lamb_c_sector* a, int32_t na, const lamb_c_se
   lamb_oracle_result* R = (lamb_oracle_result*)calloc(1, sizeof(*R));
   R->n = Sm * Sn;
   R->s = (csec*)calloc((size_t)R->n > 0 ? R->n : 1, sizeof(csec));
-  R->has_stacks = (row_stride == 1);
+  R->has_stacks = (row_stride == 1) && !(flags & ORACLE_NO_STACKS);
   int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
 
   for (int32_t m = 1; m <= Sm; ++m)
@@ -394,5 +394,80 @@ int32_t lamb_oracle_free(lamb_oracle_result* r) {
   }
   free(r->s);
   free(r);
+  return 0;
+}
+
+/* Compares a device result (downloaded sectors `got`) with an oracle result
+ * computed WITHOUT the result filter: a reference block is expected in `got`
+ * iff !(|C_ij|_F < eps) (all blocks when eps <= 0).  Counts pattern
+ * mismatches (expected blocks missing, unexpected blocks present, block
+ * sizes), sums |got - ref|^2 and |ref|^2 over the expected blocks, and returns
+ * the smallest | |C_ij|_F - eps | / eps over all reference blocks (how close
+ * any block sits to the filter threshold; +inf when eps <= 0). */
+int32_t lamb_oracle_compare(const lamb_oracle_result* r, const lamb_c_sector* got, int32_t n_got, double eps,
+                            int32_t n_threads, int64_t* n_mismatch, double* num, double* den, double* min_gap) {
+  if (!r || (!got && n_got) || !n_mismatch || !num || !den || !min_gap) return 1;
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+  int64_t mis = 0;
+  double sn = 0.0, sd = 0.0, gap = INFINITY;
+  for (int s = 0; s < r->n; ++s) {
+    const csec* C = &r->s[s];
+    const int g = find_sector(got, n_got, C->sr, C->sc);
+    if (g < 0) {
+      if (C->n_blks) mis += C->n_blks;
+      continue;
+    }
+    const lamb_c_sector* G = &got[g];
+    if (G->n_rows != C->nr || G->n_cols != C->nc) { mis += 1; continue; }
+    int64_t m_loc = 0;
+    double n_loc = 0.0, d_loc = 0.0, g_loc = INFINITY;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 16) reduction(+ : m_loc, n_loc, d_loc) reduction(min : g_loc)
+    for (int32_t l = 0; l < C->nr; ++l) {
+      int64_t q = G->row_p[l];
+      const int64_t qe = G->row_p[l + 1];
+      const int bi = C->rbs[l];
+      for (int64_t b = C->row_p[l]; b < C->row_p[l + 1]; ++b) {
+        const int32_t col = C->col_i[b];
+        const int64_t sz = (int64_t)bi * C->cbs[col - 1];
+        const double* rv = C->data + C->extents[2 * b] - 1;
+        const double nrm = lamb_oracle_block_norm(rv, sz);
+        if (eps > 0) {
+          const double gp = fabs(nrm - eps) / eps;
+          if (gp < g_loc) g_loc = gp;
+        }
+        const int keep = !(eps > 0) || !(nrm < eps);
+        while (q < qe && G->col_i[q] < col) { ++m_loc; ++q; }  /* unexpected block in got */
+        const int present = q < qe && G->col_i[q] == col;
+        if (keep != present) ++m_loc;
+        if (present) {
+          const int64_t glen = G->extents[2 * q + 1] - G->extents[2 * q] + 1;
+          if (glen != sz) ++m_loc;
+          else if (keep) {
+            const double* gv = G->data + G->extents[2 * q] - 1;
+            for (int64_t e = 0; e < sz; ++e) {
+              const double d = gv[e] - rv[e];
+              n_loc += d * d;
+              d_loc += rv[e] * rv[e];
+            }
+          }
+          ++q;
+        }
+      }
+      m_loc += qe - q;  /* trailing unexpected blocks */
+    }
+    mis += m_loc;
+    sn += n_loc;
+    sd += d_loc;
+    if (g_loc < gap) gap = g_loc;
+  }
+  for (int i = 0; i < n_got; ++i) {  /* sectors the reference does not have */
+    int found = 0;
+    for (int s = 0; s < r->n && !found; ++s) found = r->s[s].sr == got[i].subset_row && r->s[s].sc == got[i].subset_col;
+    if (!found) mis += got[i].n_blks;
+  }
+  *n_mismatch = mis;
+  *num = sn;
+  *den = sd;
+  *min_gap = gap;
   return 0;
 }

@@ -48,6 +48,8 @@ typedef struct lamb_oracle_result lamb_oracle_result;
 /* flags: LAMB_GPU_NO_PRODUCT_FILTER / LAMB_GPU_NO_RESULT_FILTER from lamb_gpu.h;
  * ORACLE_LONG_DOUBLE accumulates in long double (error reference). */
 #define ORACLE_LONG_DOUBLE 0x100u
+/* ORACLE_NO_STACKS: keep no stack entries (full-size runs; saves 48 bytes per product). */
+#define ORACLE_NO_STACKS 0x200u
 /* n_threads <= 0: use all OpenMP threads. row_stride > 1 computes only every
  * row_stride-th row of each C sector (a bounded sample for timing). */
 int32_t lamb_oracle_multiply(const lamb_c_sector* a, int32_t na, const lamb_c_sector* b, int32_t nb,
@@ -63,6 +65,12 @@ int32_t lamb_oracle_stats(const lamb_oracle_result* r, int64_t* n_products, int6
  * without row sampling. */
 int32_t lamb_oracle_stacks(const lamb_oracle_result* r, int64_t* entries, int64_t* n_entries);
 int32_t lamb_oracle_free(lamb_oracle_result* r);
+/* Whole-result check of a device C against a result computed with
+ * LAMB_GPU_NO_RESULT_FILTER: pattern mismatches under the filter rule at eps,
+ * sum of squared differences and of squared reference values over the kept
+ * blocks, and the closest relative distance of any block norm to eps. */
+int32_t lamb_oracle_compare(const lamb_oracle_result* r, const lamb_c_sector* got, int32_t n_got, double eps,
+                            int32_t n_threads, int64_t* n_mismatch, double* num, double* den, double* min_gap);
 /* Block norm exactly as the GPU computes it. */
 double lamb_oracle_block_norm(const double* x, int64_t n);
 

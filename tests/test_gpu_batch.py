@@ -39,6 +39,32 @@ def test_batch_of_uneven_instances(gpu_ctx):
     batch.destroy()
 
 
+def test_batch_refuses_changed_operands(gpu_ctx):
+    """The graph holds the operands' device pointers: once C is re-multiplied
+    (new layout) or an operand is destroyed, execute returns lamb_wrong_args
+    before launching anything."""
+    from lamb_b200.gpu import LambError
+    g = WaterGeometry(16, None, 5.0, seed=2)
+    a, b = g.matrix(1), g.matrix(2)
+    da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+    dc = gpu_ctx.create_like(da)
+    batch = gpu_ctx.batch([da], [db], [dc], eps=1e-10)
+    batch.execute()
+    gpu_ctx.multiply(da, db, dc, 1e-10)       # replaces C's buffers
+    with pytest.raises(LambError) as e:
+        batch.execute()
+    assert e.value.type == 100
+    batch.destroy()
+    batch = gpu_ctx.batch([da], [db], [dc], eps=1e-10)
+    db.destroy()
+    with pytest.raises(LambError) as e:
+        batch.execute()
+    assert e.value.type == 100
+    batch.destroy()
+    dc.destroy()
+    da.destroy()
+
+
 def test_batch_rejects_shared_outputs(gpu_ctx):
     g = WaterGeometry(16, None, 5.0, seed=1)
     a = g.matrix(1)

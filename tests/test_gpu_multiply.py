@@ -264,18 +264,21 @@ def _rows_of(m: LambMatrix, stride: int):
     return out
 
 
-def test_water6144_cut8_sampled_rows(gpu_ctx):
-    """Full-size workload: GPU C against the oracle on every 61st row."""
+def test_water6144_cut8_whole_product(gpu_ctx):
+    """Full-size workload (6,144 waters, cutoff 8 A, eps 1e-10), every row:
+    the GPU C (both filters on) against the oracle's whole product.  The
+    oracle computes C without the result filter and applies the filter rule
+    while comparing, so the check also shows how close any block norm comes
+    to eps (a block within rounding of eps could flip either way)."""
     g, a, b = WATER_6144.build()
     c, st = _gpu_mult(gpu_ctx, a, b, WATER_6144.eps)
-    c.validate()
-    stride = 61
-    c_ref, st_ref = oracle.multiply(a, b, WATER_6144.eps, row_stride=stride)
-    got, ref = _rows_of(c, stride), _rows_of(c_ref, stride)
-    assert set(got) == set(ref)
-    num = sum(float(np.sum((got[k] - ref[k]) ** 2)) for k in ref)
-    den = sum(float(np.sum(ref[k] ** 2)) for k in ref)
-    assert np.sqrt(num / den) <= TOL_FP64
+    r = oracle.check_product(a, b, WATER_6144.eps, c)
+    assert r["min_rel_gap_to_eps"] > 1e-9
+    assert r["pattern_mismatches"] == 0
+    assert r["rel_frobenius_err"] <= TOL_FP64
+    assert st["n_products"] == r["n_products"]
+    assert st["n_products_skipped"] == r["n_products_skipped"]
+    assert st["flops"] == r["flops"]
     assert st["n_c_blocks"] == sum(s.n_blks for s in c.sectors)
 
 
@@ -314,9 +317,11 @@ def test_block_size_classes(gpu_ctx, blk_o, blk_h):
 
 
 @pytest.mark.parametrize("slices,tol", [(7, 1e-11), (6, 1e-9)])
-def test_mixed_precision_error(gpu_ctx, monkeypatch, slices, tol):
-    """int8 split-slice products: same pattern as FP64, error against the
-    long-double oracle within the stated bound."""
+def test_mixed_mma_sync_precision_error(gpu_ctx, monkeypatch, slices, tol):
+    """The mma.sync digit kernel (kept for shapes the tensor-core path does
+    not take): same pattern as FP64, error against the long-double oracle
+    within the stated bound."""
+    monkeypatch.setenv("LAMB_GPU_MIXED_MMA_SYNC", "1")
     monkeypatch.setenv("LAMB_GPU_MIXED_SLICES", str(slices))
     g = WaterGeometry(96, None, 7.0, seed=21)
     a, b = g.matrix(1), g.matrix(2)
@@ -328,8 +333,50 @@ def test_mixed_precision_error(gpu_ctx, monkeypatch, slices, tol):
     assert err <= tol, err
 
 
-def test_mixed_precision_random_fill(gpu_ctx, monkeypatch):
-    monkeypatch.setenv("LAMB_GPU_MIXED_SLICES", "7")
+# Tensor-core path (tcgen05 kind::i8 on cluster tiles, six base-254 digits):
+# the bound the configuration states for the mixed multiply.
+TOL_MIXED = 1e-11
+
+
+@pytest.mark.parametrize("n_mol,cutoff,blk_o,blk_h", [(96, 7.0, 13, 5), (64, 6.0, 23, 5), (40, 6.0, 40, 7),
+                                                      (30, 5.0, 3, 1), (200, 8.0, 13, 5)])
+def test_mixed_tensor_core_error(gpu_ctx, n_mol, cutoff, blk_o, blk_h):
+    """Same C pattern as the oracle, error against the long-double oracle
+    within 1e-11, over block-size classes (1 to 40 rows) and box sizes."""
+    g = WaterGeometry(n_mol, None, cutoff, blk_o=blk_o, blk_h=blk_h, seed=21)
+    a, b = g.matrix(1), g.matrix(2)
+    c_ld, _ = oracle.multiply(a, b, 1e-10, oracle.LONG_DOUBLE)
+    _no_borderline(c_ld, 1e-10)
+    c, st = _gpu_mult(gpu_ctx, a, b, 1e-10, gpu.MIXED)
+    assert st["mixed_slices"] == 6
+    c.validate()
+    assert_same_pattern(c, c_ld)
+    err = rel_frobenius_error(c, c_ld)
+    assert err <= TOL_MIXED, err
+
+
+def test_mixed_tensor_core_keeps_filtered_pattern(gpu_ctx):
+    """With an eps that filters products, C's pattern is the filtered one
+    (bit-exact with the oracle); its blocks carry every product, the
+    filtered ones included (each below eps), so the values are checked
+    against the unfiltered product on that pattern."""
+    g = WaterGeometry(48, None, 6.0, seed=8)
+    a, b = g.matrix(1), g.matrix(2)
+    eps = 1e-3
+    c_ref, st_ref = oracle.multiply(a, b, eps, oracle.NO_RESULT_FILTER)
+    assert st_ref["n_products_skipped"] > 0
+    c, st = _gpu_mult(gpu_ctx, a, b, eps, gpu.MIXED | gpu.NO_RESULT_FILTER)
+    assert_same_pattern(c, c_ref)
+    assert st["n_products"] == st_ref["n_products"] and st["flops"] == st_ref["flops"]
+    full, _ = oracle.multiply(a, b, 0.0, oracle.LONG_DOUBLE)
+    fv, cv = block_values(full), block_values(c)
+    num = sum(float(np.sum((cv[k] - fv[k]) ** 2)) for k in cv)
+    den = sum(float(np.sum(fv[k] ** 2)) for k in cv)
+    assert np.sqrt(num / den) <= TOL_MIXED
+
+
+def test_mixed_precision_random_fill(gpu_ctx):
+    """Zero-size and 1-3 element blocks, fill 0.7, no filter."""
     a = random_fill_matrix(5)
     b = _with_values(a, 9)
     c_ld, _ = oracle.multiply(a, b, 0.0, oracle.LONG_DOUBLE)

@@ -133,3 +133,35 @@ def _from_npz(z, p):
         secs.append(Sector(int(z[q + "sr"]), int(z[q + "sc"]), z[q + "rbs"], z[q + "cbs"], z[q + "row_p"],
                            z[q + "col_i"], z[q + "extents"], z[q + "data"]))
     return LambMatrix(secs)
+
+
+def test_whole_product_check_accepts_itself_and_catches_planted_mistakes():
+    """oracle.check_product (used for the whole 6,144-water comparison on the
+    GPU): the oracle's own filtered result passes; a changed value, a dropped
+    block and an extra block are each caught.  The mistakes are planted in a
+    copy of the oracle's result, on the CPU."""
+    g = WaterGeometry(40, None, 5.0, seed=21)
+    a, b = g.matrix(1), g.matrix(2)
+    eps = 0.1
+    c, st = oracle.multiply(a, b, eps)
+    assert st["n_c_blocks_dropped"] > 0  # the filter rule is exercised
+    ok = oracle.check_product(a, b, eps, c)
+    assert ok["pattern_mismatches"] == 0 and ok["rel_frobenius_err"] == 0.0
+    assert ok["n_products"] == st["n_products"] and ok["min_rel_gap_to_eps"] > 0
+
+    def copy(m):
+        return LambMatrix([Sector(s.subset_row, s.subset_col, s.row_blk_sizes.copy(), s.col_blk_sizes.copy(),
+                                  s.row_p.copy(), s.col_i.copy(), s.extents.copy(), s.data.copy())
+                           for s in m.sectors])
+    bad = copy(c)
+    bad.sectors[0].data[5] += 1e-6
+    r = oracle.check_product(a, b, eps, bad)
+    assert r["pattern_mismatches"] == 0 and r["rel_frobenius_err"] > 1e-12
+    # drop the first block of sector 0 (row_p shifts down by one after row 0's first block)
+    s0 = c.sectors[0]
+    bad = copy(c)
+    t = bad.sectors[0]
+    bad.sectors[0] = Sector(t.subset_row, t.subset_col, t.row_blk_sizes, t.col_blk_sizes,
+                            np.maximum(t.row_p - 1, 0), t.col_i[1:], t.extents[1:], t.data)
+    assert oracle.check_product(a, b, eps, bad)["pattern_mismatches"] >= 1
+    assert s0.n_blks > 1

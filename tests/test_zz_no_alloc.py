@@ -91,6 +91,37 @@ def test_noalloc_trace_product_matches_allocating_entry_point(gpu_ctx):
     dy.destroy()
 
 
+def test_noalloc_empty_y_with_null_arrays(gpu_ctx):
+    """Y without blocks may come with null arrays: the trace is 0."""
+    import torch
+    g = WaterGeometry(12, None, 4.0, seed=5)
+    x = g.matrix(1)
+    sx, kx = _device_csr(x)
+    y = DCSR(sx.n_cols, sx.n_rows, 0, None, None, None, None, None, None)
+    torch.cuda.synchronize()
+    out = C.c_double(float("nan"))
+    assert _noalloc()(C.byref(sx), C.byref(y), None, C.byref(out)) == 0
+    assert out.value == 0.0
+
+
+def test_noalloc_rejects_mismatched_blocking(gpu_ctx):
+    """Same pattern, O blocks of 13 in X and 23 in Y: every Y_ji has the wrong
+    shape, so the call skips the blocks and returns lamb_wrong_args."""
+    import torch
+    x = WaterGeometry(12, None, 4.0, seed=5, blk_o=13).matrix(1)
+    y = WaterGeometry(12, None, 4.0, seed=5, blk_o=23).matrix(2)
+    sx, kx = _device_csr(x)
+    sy, ky = _device_csr(y)
+    torch.cuda.synchronize()
+    out = C.c_double(0.0)
+    st = _noalloc()(C.byref(sx), C.byref(sy), None, C.byref(out))
+    assert gpu.lib().lamb_gpu_status_type(st) == 100
+    # the flag does not stick: a matching pair right after succeeds
+    sy2, ky2 = _device_csr(WaterGeometry(12, None, 4.0, seed=5, blk_o=13).matrix(2))
+    torch.cuda.synchronize()
+    assert _noalloc()(C.byref(sx), C.byref(sy2), None, C.byref(out)) == 0
+
+
 def test_noalloc_rejects_oversized_input():
     x = DCSR(1, 1, (1 << 20) + 1, None, None, None, None, None, None)
     out = C.c_double(0.0)
