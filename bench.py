@@ -36,6 +36,9 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 METRIC = "block-SpGEMM GFLOP/s (FP64-equivalent), LAMB sector multiply"
+# Every CPU timing (the cpu_baseline leg and the reference arm) runs the
+# oracle on every CPU_ROW_STRIDE-th C block row of the same workload.
+CPU_ROW_STRIDE = 6
 
 
 def parse():
@@ -48,16 +51,35 @@ def parse():
                    choices=["water6144_cut8", "water1536_cut7", "water192_cut6", "batch64", "mcweeny384",
                             "adjoint96"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-positions", action="store_true", help="order work from the block pattern only")
-    p.add_argument("--mixed-steps", type=int, default=2, help="timed steps of the int8-slice path (0 skips it)")
+    p.add_argument("--mixed-steps", type=int, default=3, help="timed steps of the int8-slice path (0 skips it)")
+    p.add_argument("--no-full-check", action="store_true", help="skip the whole-product check against the oracle")
+    p.add_argument("--batch-steps", type=int, default=3, help="timed full runs of the 64-box batch (0 skips it)")
     return p.parse_args()
 
 
 def workload(name):
     from lamb_b200 import gen
     return {"water6144_cut8": gen.WATER_6144, "water1536_cut7": gen.WATER_1536, "water192_cut6": gen.WATER_192}[name]
+
+
+def workload_config(wl, g) -> dict:
+    """The workload (identical in both arms)."""
+    return {"workload": wl.name, "n_mol": wl.n_mol, "n_atoms": int(g.n_atoms), "box": wl.box, "cutoff": wl.cutoff,
+            "eps": wl.eps, "seeds": {"geometry": wl.geom_seed, "A": wl.seed_a, "B": wl.seed_b},
+            "blocks": {"O": wl.blk_o, "H": wl.blk_h}}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
 
 
 def algorithmic_bytes(a, b, c) -> int:
@@ -136,26 +158,27 @@ def measured_peaks():
 
 
 def committed_traffic(kernel, wl):
-    path = os.path.join(REPO, "profiles", f"{kernel}_{wl}.traffic.json")
+    """DRAM bytes per multiply of `kernel` at workload `wl`, from the
+    committed summary profiles/<kernel>_traffic.json (a small-case ncu capture
+    and its scaling to each workload); None when absent."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            return json.load(f)["per_multiply_bytes"].get(wl)
     except Exception:
         return None
 
 
-def cpu_sample(a, b, eps, seconds, threads):
-    """Times the oracle on every s-th C row, s picked for about `seconds`."""
+def cpu_sample(a, b, eps, threads, reps=1):
+    """Times the oracle on every CPU_ROW_STRIDE-th C row (`reps` runs)."""
     import oracle
-    probe = 997
-    t = time.perf_counter()
-    _, st = oracle.multiply(a, b, eps, threads=threads, row_stride=probe)
-    dt = max(time.perf_counter() - t, 1e-3)
-    stride = max(1, int(probe * dt / seconds))
-    t = time.perf_counter()
-    c, st = oracle.multiply(a, b, eps, threads=threads, row_stride=stride)
-    dt = time.perf_counter() - t
-    return c, st, dt, stride
+    fl, dt, c = 0.0, 0.0, None
+    for _ in range(reps):
+        t = time.perf_counter()
+        c, st = oracle.multiply(a, b, eps, threads=threads, row_stride=CPU_ROW_STRIDE)
+        dt += time.perf_counter() - t
+        fl += st["flops"]
+    return c, fl, dt
 
 
 def rows_of(m, stride):
@@ -207,34 +230,77 @@ def matrix_bytes(m):
 
 def run_reference(args):
     """CPU arm: the oracle (the reference's multiply is a stub and its Fortran
-    does not build here), all host cores, a bounded row sample per step."""
+    does not build here), all host threads, every CPU_ROW_STRIDE-th C block
+    row of the same workload per step.  Inputs come from the same generator
+    (liblamb_gen.so) outside the timed region."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     wl = workload(args.workload)
     g, a, b = wl.build()
     threads = os.cpu_count() or 1
-    per_step = max(2.0, min(20.0, 150.0 / max(args.steps + args.warmup, 1)))
     import oracle
-    _, _, dt, stride = cpu_sample(a, b, wl.eps, per_step, threads)
     for _ in range(args.warmup):
-        oracle.multiply(a, b, wl.eps, threads=threads, row_stride=stride)
+        oracle.multiply(a, b, wl.eps, threads=threads, row_stride=CPU_ROW_STRIDE)
     fl, tt = 0.0, 0.0
     for _ in range(args.steps):
-        t = time.perf_counter()
-        _, st = oracle.multiply(a, b, wl.eps, threads=threads, row_stride=stride)
-        tt += time.perf_counter() - t
-        fl += st["flops"]
+        _, f, dt = cpu_sample(a, b, wl.eps, threads)
+        tt += dt
+        fl += f
     v = fl / tt / 1e9
-    sample = f"every {stride}-th C block row of {wl.name} per step"
+    sample = f"every {CPU_ROW_STRIDE}th C block row of {wl.name} per step ({fl / args.steps / 1e9:.1f} GFLOP)"
+    cpu = {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port", "sample": sample, "cpu": cpu_model()}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wl.name, "n_mol": wl.n_mol, "box": wl.box, "cutoff": wl.cutoff, "eps": wl.eps},
-            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port", "sample": sample},
+            "config": workload_config(wl, g),
+            "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "oracle restatement (the reference's sector_multiply is a stub and needs gfortran+MPI)"}
+            "note": "oracle restatement in C + OpenMP (the reference's sector_multiply is a stub and needs "
+                    "gfortran+MPI); inputs from liblamb_gen.so, built outside the timed region"}
     print(json.dumps(line), flush=True)
+
+
+def run_mixed_leg(ctx, lib, local, da, db, dc, wl, args, flops, ms_fp64):
+    """The mixed multiply (int8 digit products on the tensor cores, FP64
+    recombination) on the FP64 leg's inputs: time per phase, error against
+    the FP64 result, and the tensor-core roofline of the tile kernel."""
+    import ctypes
+    from lamb_b200 import gpu
+    dcm = ctx.create_like(da)
+    ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED)  # warm-up: pool growth
+    mst = [ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED) for _ in range(args.mixed_steps)]
+    rel = ctx.diff_frobenius(dcm, dc) / ctx.frobenius(dc)
+    dcm.destroy()
+    mean = lambda k: statistics.mean(x[k] for x in mst)
+    ms_m, ms_num = mean("ms_total"), mean("ms_numeric")
+    s_m = int(mst[-1]["mixed_slices"])
+    out = {"value": flops / (ms_m * 1e-3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms_m, "steps": args.mixed_steps,
+           "phases_ms": {"exponents_and_pattern": mean("ms_symbolic") - mean("ms_prepare"),
+                         "panels_tiles_inner_lists": mean("ms_prepare"), "numeric": ms_num,
+                         "result_filter": mean("ms_filter")},
+           "ms_symbolic": mean("ms_symbolic"), "ms_numeric": ms_num, "slices": s_m,
+           "rel_frobenius_err_vs_fp64": rel, "ms_ratio_vs_fp64": ms_m / ms_fp64}
+    t_ops = mst[-1]["tensor_ops"]
+    if t_ops > 0:
+        f = lib.lamb_probe_int8_tcgen05_tops
+        f.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+        peak = ctypes.c_double()
+        ctx.check(f(local, 64, 5, ctypes.byref(peak)))
+        achieved = t_ops / (ms_num * 1e-3) / 1e12
+        out["path"] = ("tcgen05.mma kind::i8 (M=128, N=64, K=32) on 128x64 spatial cluster tiles, six base-254 "
+                       "digits per operand, 21 digit-pair products into six int32 TMEM level accumulators, FP64 "
+                       "recombination")
+        out["roofline"] = {"bound": "tensor", "kernel": "k_tc_tiles", "achieved": achieved, "peak": peak.value,
+                           "unit": "TOP/s (int8)", "frac": achieved / peak.value,
+                           "peak_source": "tcgen05 kind::i8 N=64 throughput probe on this GPU in this run",
+                           "tensor_ops_per_multiply": t_ops,
+                           "useful_fraction": flops * s_m * (s_m + 1) / 2 / t_ops,
+                           "note": "executed ops include the zero padding of the cluster tiles; useful_fraction = "
+                                   "FP64-equivalent flops x 21 digit pairs / executed ops"}
+    else:
+        out["path"] = "int8 digit slices through mma.m16n8k32.s8 (the tile limits of the tensor-core kernel were exceeded)"
+    return out
 
 
 def run_ours(args):
@@ -299,37 +365,14 @@ def run_ours(args):
     alg_bytes = algorithmic_bytes(a, b, c_host)
     peaks, peak_kind = measured_peaks()
     achieved_tf = flops / (ms_num * 1e-3) / 1e12
-    # the int8-slice path on the same inputs, its error taken against the FP64 result
+    # the mixed path on the same inputs, its error taken against the FP64 result
     mixed = None
     if args.mixed_steps > 0:
-        dcm = ctx.create_like(da)
-        ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED)
-        mst = [ctx.multiply(da, db, dcm, wl.eps, gpu.MIXED) for _ in range(args.mixed_steps)]
-        ms_m = statistics.mean(s["ms_total"] for s in mst)
-        rel = ctx.diff_frobenius(dcm, dc) / ctx.frobenius(dc)
-        lib.lamb_probe_int8_tops.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
-        ipeak = ctypes.c_double()
-        ctx.check(lib.lamb_probe_int8_tops(local, 5, ctypes.byref(ipeak)))
-        # bf16 slices with FP32 accumulation: the alternative slice format (context only)
-        lib.lamb_probe_bf16_tflops.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
-        hpeak = ctypes.c_double()
-        ctx.check(lib.lamb_probe_bf16_tflops(local, 5, ctypes.byref(hpeak)))
-        s_m = int(mst[-1]["mixed_slices"])
-        ms_mn = statistics.mean(s["ms_numeric"] for s in mst)
-        # every FP64-equivalent flop is s(s+1)/2 int8 plane-product ops (digit pairs p + q <= s - 1)
-        int8_tops = flops * (s_m * (s_m + 1) // 2) / (ms_mn * 1e-3) / 1e12
-        mixed = {"value": flops / (ms_m * 1e-3) / 1e9, "unit": "GFLOP/s", "ms_per_step": ms_m,
-                 "roofline": {"bound": "tensor", "kernel": "k_mixed", "achieved": int8_tops, "peak": ipeak.value,
-                              "unit": "TOP/s (int8)", "frac": int8_tops / ipeak.value,
-                              "peak_source": "mma.m16n8k32.s8 probe measured on this GPU in this run",
-                              "ops": "FP64-equivalent flops x s(s+1)/2 digit-pair products"},
-                 "ms_numeric": statistics.mean(s["ms_numeric"] for s in mst),
-                 "ms_symbolic": statistics.mean(s["ms_symbolic"] for s in mst),
-                 "slices": int(mst[-1]["mixed_slices"]), "steps": args.mixed_steps,
-                 "rel_frobenius_err_vs_fp64": rel, "ms_ratio_vs_fp64": ms_m / ms_tot,
-                 "path": "int8 digit slices, mma.m16n8k32.s8, exact int32 planes, FP64 recombination",
-                 "bf16_mma_sync_peak_tflops": hpeak.value}
-        dcm.destroy()
+        mixed = run_mixed_leg(ctx, lib, local, da, db, dc, wl, args, flops, ms_tot)
+    # cfg2: the 64-box batch, full multiply per step (rank 0 of a single-GPU run)
+    batch = None
+    if world == 1 and args.batch_steps > 0:
+        batch = batch_leg(ctx, args, args.batch_steps, 2)
     # e2e through the C ABI with page-locked host buffers
     pa, pb = pin_matrix(a), pin_matrix(b)
     c_out = dc.download(pinned=True)
@@ -358,26 +401,38 @@ def run_ours(args):
     e2e_value = flops * world / float(e2e_t.item()) / 1e9
     cpu = None
     err = None
+    full = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        c_ref, st_ref, dt, stride = cpu_sample(a, b, wl.eps, args.cpu_seconds, threads)
-        cpu = {"value": st_ref["flops"] / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
-               "sample": f"every {stride}-th C block row of {wl.name} ({st_ref['flops'] / 1e9:.1f} GFLOP, "
-                         f"{dt:.1f} s)"}
-        err = sampled_error(c_host, c_ref, stride)
+        c_ref, fl_ref, dt = cpu_sample(a, b, wl.eps, threads, reps=2)
+        cpu = {"value": fl_ref / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+               "sample": f"every {CPU_ROW_STRIDE}th C block row of {wl.name}, twice ({fl_ref / 1e9:.1f} GFLOP, "
+                         f"{dt:.1f} s)", "cpu": cpu_model()}
+        err = sampled_error(c_host, c_ref, CPU_ROW_STRIDE)
+        del c_ref
+    if rank == 0 and world == 1 and not args.no_full_check:
+        # every row of the FP64 result against the oracle (pattern under the
+        # filter rule, relative Frobenius error), outside the timed regions
+        import oracle
+        t = time.perf_counter()
+        full = oracle.check_product(a, b, wl.eps, c_host)
+        full["seconds"] = time.perf_counter() - t
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water boxes)",
-            "config": {"workload": wl.name, "n_mol": wl.n_mol, "n_atoms": g.n_atoms, "box": wl.box,
-                       "cutoff": wl.cutoff, "eps": wl.eps, "path": "plain FP64 (DMMA)", "row_order": "pattern (Cuthill-McKee)" if args.no_positions else "Morton (atom coordinates)",
-                       "l2": "inputs 2x1.9 GB exceed L2; no flush", "parallelism": f"replicas x{world}"},
+            "config": workload_config(wl, g),
+            "setup": {"path": "plain FP64 (DMMA)",
+                      "row_order": "pattern (Cuthill-McKee)" if args.no_positions else "Morton (atom coordinates)",
+                      "l2": "inputs 2x1.9 GB exceed L2; no flush", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "tensor", "kernel": "k_stacked", "achieved": achieved_tf,
                          "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak,
                          "peak_source": "FP64 DMMA probe measured on this GPU in this run",
                          "traffic": committed_traffic("k_stacked", wl.name),
-                         "flops_per_launch": flops, "ms_per_launch": ms_num},
+                         "traffic_scope": "DRAM bytes of one multiply's k_stacked launches (all row chunks), "
+                                          "scaled from the committed small-case capture; null when none",
+                         "flops_per_multiply": flops, "ms_per_multiply": ms_num},
             "roofline_hbm": {"bound": "hbm", "achieved": alg_bytes / (ms_tot * 1e-3) / 1e9,
                              "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                              "frac": alg_bytes / (ms_tot * 1e-3) / 1e9 / peaks.get("hbm_gbs"),
@@ -387,7 +442,9 @@ def run_ours(args):
                     "ms_per_step": statistics.mean(t_e2e) * 1e3},
             "cpu_baseline": cpu,
             "max_rel_err_vs_oracle": err,
+            "full_check_vs_oracle": full,
             "mixed": mixed,
+            "batch": batch,
             "stats": {k: stats[-1][k] for k in ("n_products", "n_c_blocks", "ms_symbolic", "ms_numeric", "ms_total")},
             # timed region per step minus the multiply's own device time: host-side
             # stalls between and inside the multiplies (the GPU idles meanwhile)
@@ -403,15 +460,14 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_batch(args):
-    """64 uneven independent water boxes, one graph-replayed persistent launch per step."""
+def batch_leg(ctx, args, steps, warmup):
+    """cfg2: 64 uneven independent water boxes.  Every timed step is a full
+    run of the batch: symbolic phase of every instance, one graph-replayed
+    persistent numeric launch over the global queue, result filter of every
+    instance (lamb_gpu_batch_run with LAMB_GPU_BATCH_FULL)."""
     import torch
-    from lamb_b200 import build
-    build.build_all()
     from lamb_b200.gen import batch_instances
-    from lamb_b200.gpu import Context
     wls = batch_instances()
-    ctx = Context(0)
     devs = []
     t0 = time.perf_counter()
     for wl in wls:
@@ -425,28 +481,46 @@ def run_batch(args):
     t0 = time.perf_counter()
     batch = ctx.batch([d[0] for d in devs], [d[1] for d in devs], [d[2] for d in devs], eps=1e-10)
     t_create = time.perf_counter() - t0
-    clk = Clocks(0)
-    for _ in range(args.warmup):
-        st = batch.execute()
+    for _ in range(warmup):
+        batch.run_full()
     torch.cuda.synchronize()
+    clk = Clocks(ctx.device)
     clk.mark()
-    ms = []
-    for _ in range(args.steps):
-        ms.append(batch.execute()["ms_total"])
+    sts = [batch.run_full() for _ in range(steps)]
     clocks = clk.stop()
-    st = batch.execute()
-    value = st["flops"] / (statistics.mean(ms) * 1e-3) / 1e9
-    line = {"metric": METRIC + " (batched)", "value": value, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": statistics.mean(ms), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water boxes)",
-            "config": {"workload": "batch64: 64 boxes of 96-1536 waters (log-uniform, seed 3), cutoffs U[5,9] A, "
-                                   "O 23 / H 5 in half, O 13 / H 5 in the rest", "eps": 1e-10,
-                       "graph": "captured once, replayed per step", "tuned": batch.config()},
-            "stats": {"flops": st["flops"], "n_products": st["n_products"], "n_c_blocks": st["n_c_blocks"],
-                      "build_s": t_build, "create_s": t_create},
-            "gpu_launches": int(st["kernel_launches"]) * args.steps, "clocks": clocks}
-    print(json.dumps(line), flush=True)
+    mean = lambda k: statistics.mean(x[k] for x in sts)
+    st = sts[-1]
+    out = {"metric": METRIC + " (batched, full multiply per step)", "value": st["flops"] / (mean("ms_total") * 1e-3) / 1e9,
+           "unit": "GFLOP/s", "steps": steps, "warmup": warmup, "ms_per_step": mean("ms_total"),
+           "phases_ms": {"symbolic": mean("ms_symbolic"), "numeric_graph_replay": mean("ms_numeric"),
+                         "result_filter": mean("ms_filter")},
+           "numeric_only_gflops": st["flops"] / (mean("ms_numeric") * 1e-3) / 1e9,
+           "config": {"workload": "batch64: 64 boxes of 96-1536 waters (log-uniform, seed 3), cutoffs U[5,9] A, "
+                                  "O 23 / H 5 in half, O 13 / H 5 in the rest", "eps": 1e-10,
+                      "graph": "numeric launch captured once, replayed per step", "tuned": batch.config()},
+           "stats": {"flops": st["flops"], "n_products": st["n_products"], "n_c_blocks": st["n_c_blocks"],
+                     "n_c_blocks_dropped": st["n_c_blocks_dropped"], "build_s": t_build, "create_s": t_create},
+           "gpu_launches_per_step": int(st["kernel_launches"]), "clocks": clocks}
     batch.destroy()
+    for m in devs:
+        for x in m:
+            x.destroy()
+    return out
+
+
+def run_batch(args):
+    """64 uneven independent water boxes, the standalone line."""
+    from lamb_b200 import build
+    build.build_all()
+    from lamb_b200.gpu import Context
+    ctx = Context(0)
+    out = batch_leg(ctx, args, args.steps, args.warmup)
+    line = {"metric": out.pop("metric"), "value": out.pop("value"), "unit": "GFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": out.pop("ms_per_step"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded water boxes)", "config": out.pop("config"),
+            "gpu_launches": out["gpu_launches_per_step"] * args.steps, **out}
+    print(json.dumps(line), flush=True)
     ctx.close()
 
 

@@ -140,6 +140,9 @@ typedef struct lamb_gpu_mult_stats {
   double ms_prepare;         /* part of ms_symbolic spent preparing operands
                                 (mixed: digit planes / panels; FP64: 0)       */
   double ms_filter;          /* device time of the result filter              */
+  double tensor_ops;         /* mixed, tensor-core path: int8 multiply-add ops
+                                the tile kernel executed (2 per MAC, padding
+                                of the cluster tiles included); else 0       */
 } lamb_gpu_mult_stats;
 
 typedef struct lamb_gpu_ctx lamb_gpu_ctx;
@@ -335,10 +338,22 @@ LAMB_API int32_t lamb_gpu_multiply_adjoint(lamb_gpu_ctx* ctx, lamb_gpu_matrix a,
 typedef struct lamb_gpu_batch lamb_gpu_batch;
 LAMB_API int32_t lamb_gpu_batch_create(lamb_gpu_ctx* ctx, const lamb_gpu_matrix* a, const lamb_gpu_matrix* b,
                               const lamb_gpu_matrix* c, int32_t n, double eps, lamb_gpu_batch** batch);
-/* Runs the batch once (first call captures the graph; later calls replay).
- * Product-filter decisions and C patterns are fixed at creation; executions
- * recompute the block products from the current A/B values. */
+/* Runs the batch's numeric phase once (first call captures the graph; later
+ * calls replay).  Product-filter decisions and C patterns are those of the
+ * last full run (or of creation); the block products are recomputed from the
+ * current A/B values.  Same as lamb_gpu_batch_run(batch, 0, stats). */
 LAMB_API int32_t lamb_gpu_batch_execute(lamb_gpu_batch* batch, lamb_gpu_mult_stats* stats);
+/* With LAMB_GPU_BATCH_FULL: the whole multiply of every instance -- symbolic
+ * phase from the current values (C patterns, stacks, work queue), the
+ * graph-replayed persistent numeric launch (captured again only when the
+ * queue's length changed), and the result filter at the batch's eps; the
+ * statistics give ms_symbolic, ms_numeric, ms_filter and ms_total for the
+ * three parts.  Without it, as lamb_gpu_batch_execute. */
+#define LAMB_GPU_BATCH_FULL 1u
+LAMB_API int32_t lamb_gpu_batch_run(lamb_gpu_batch* batch, uint32_t flags, lamb_gpu_mult_stats* stats);
+/* Queue order the autotuner picked: 0 instance-major (largest instance
+ * first), 1 grouped by C block shape. */
+LAMB_API int32_t lamb_gpu_batch_queue_order(const lamb_gpu_batch* batch, int32_t* by_shape);
 /* Launch shape the autotuner picked at creation: warps per CTA, stack entries
  * per column-table chunk, work items per queue fetch.  The choice is cached
  * per problem signature in the process and, when LAMB_GPU_AUTOTUNE_CACHE

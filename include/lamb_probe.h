@@ -22,6 +22,12 @@ LAMB_API int32_t lamb_probe_int8_tops(int32_t device, int32_t reps, double* tops
  * through mma.sync), the alternative slice format; writes TFLOP/s.  Allocates
  * 4 bytes per thread of the grid. */
 LAMB_API int32_t lamb_probe_bf16_tflops(int32_t device, int32_t reps, double* tflops);
+/* int8 throughput of the 5th-generation tensor cores as the mixed multiply's
+ * tile kernel drives them: one CTA per SM issues tcgen05.mma kind::i8
+ * (M = 128, K = 32, N = n: 64, the kernel's shape, or 256, the widest)
+ * from shared memory into tensor-memory accumulators; best of `reps`
+ * launches, TOP/s (1 op = 1 multiply or 1 add).  Allocates 4 bytes. */
+LAMB_API int32_t lamb_probe_int8_tcgen05_tops(int32_t device, int32_t n, int32_t reps, double* tops);
 #ifdef __cplusplus
 }
 #endif

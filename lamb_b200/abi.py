@@ -36,7 +36,7 @@ class MultStats(C.Structure):
         ("n_c_blocks", C.c_int64), ("n_c_blocks_dropped", C.c_int64),
         ("flops", C.c_double), ("ms_symbolic", C.c_double), ("ms_numeric", C.c_double), ("ms_total", C.c_double),
         ("mixed_slices", C.c_int32), ("kernel_launches", C.c_int32),
-        ("ms_prepare", C.c_double), ("ms_filter", C.c_double),
+        ("ms_prepare", C.c_double), ("ms_filter", C.c_double), ("tensor_ops", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -66,7 +66,10 @@ struct DevMatrix {
 // Gives m a new layout generation.
 void touch(DevMatrix* m);
 
-constexpr int kMaxChunks = 8;
+// Row chunks of a multiply's numeric phase: at most kMaxChunks, at least
+// kMinChunks when C has enough blocks (downloads overlap the later chunks).
+constexpr int kMaxChunks = 64;
+constexpr int kMinChunks = 8;
 
 // Roles of the context's grow-only scratch buffers (multiply temporaries).
 enum ScratchSlot : int { kScrEnt = 0, kScrWork, kScrWorkC, kScrPlaneA, kScrPlaneB, kScrSlots };

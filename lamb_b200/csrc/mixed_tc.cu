@@ -50,6 +50,7 @@
 #include <climits>
 #include <numeric>
 
+#include "lamb_probe.h"
 #include "multiply.cuh"
 
 namespace lamb {
@@ -275,7 +276,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
   if (warp < 3) {
     // ================= producers =================
     const int pt = tid;  // 0..95
-    const int kr = pt & 31, grp = pt >> 5;
+    // A stage is 32 inner rows x (8 A chunks + 4 B chunks) of 16 bytes per
+    // digit plane: 384 (row, chunk) units, four per producer thread.  Units
+    // 0..255 are A (row u / 8, chunk u % 8), 256..383 are B (row v / 4,
+    // chunk v % 4): consecutive lanes copy consecutive chunks of one panel
+    // row, so a warp reads whole 128-byte (A) or 64-byte (B) rows.
     int64_t gs = 0;      // stages issued by this CTA so far
     int64_t local = 0;
     for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
@@ -288,34 +293,34 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       for (int s = 0; s < nst; ++s, ++gs) {
         const int stg = (int)(gs % kStages);
         if (!bar_wait(&sm->bar_empty[stg], (uint32_t)(((gs / kStages) & 1) ^ 1), sm, g.err, kErrTimeoutEmpty)) break;
-        const int kk = s * kK + kr;
-        const bool valid = kk < K;
-        int64_t arow = 0, brow = 0;
-        if (valid) {
-          int lo = 0, hi = n - 1;  // last entry e with pre[e] <= kk
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (pre[mid] <= kk) lo = mid; else hi = mid - 1;
-          }
-          arow = sm->ent_a[buf][lo] + (kk - pre[lo]);
-          brow = sm->ent_b[buf][lo] + (kk - pre[lo]);
-        }
         const uint32_t sa = smem_u32(stages + (size_t)stg * kStageBytes);
         const uint32_t sb = sa + kStageA;
-        const uint32_t bytes = valid ? 16u : 0u;
-        if (grp < 2) {  // A chunks 4 grp .. 4 grp + 3 of the row
 #pragma unroll
-          for (int p = 0; p < kS; ++p) {
-            const int8_t* src = g.pan_a + p * g.plane_a + arow * 128;
-#pragma unroll
-            for (int c = 4 * grp; c < 4 * grp + 4; ++c) cp16(sa + p * kPlaneA + a_swz(kr, c), src + 16 * c, bytes);
+        for (int i = 0; i < 4; ++i) {
+          const int u = pt + kProducers * i;
+          const bool is_a = u < 256;
+          const int row = is_a ? (u >> 3) : ((u - 256) >> 2);
+          const int ch = is_a ? (u & 7) : ((u - 256) & 3);
+          const int kk = s * kK + row;
+          const bool valid = kk < K;
+          int64_t prow = 0;
+          if (valid) {
+            int lo = 0, hi = n - 1;  // last entry e with pre[e] <= kk
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (pre[mid] <= kk) lo = mid; else hi = mid - 1;
+            }
+            prow = (is_a ? sm->ent_a[buf][lo] : sm->ent_b[buf][lo]) + (kk - pre[lo]);
           }
-        } else {        // the row's 4 B chunks
+          const uint32_t bytes = valid ? 16u : 0u;
+          if (is_a) {
+            const int8_t* src = g.pan_a + prow * 128 + 16 * ch;
 #pragma unroll
-          for (int p = 0; p < kS; ++p) {
-            const int8_t* src = g.pan_b + p * g.plane_b + brow * 64;
+            for (int p = 0; p < kS; ++p) cp16(sa + p * kPlaneA + a_swz(row, ch), src + p * g.plane_a, bytes);
+          } else {
+            const int8_t* src = g.pan_b + prow * 64 + 16 * ch;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) cp16(sb + p * kPlaneB + b_swz(kr, c), src + 16 * c, bytes);
+            for (int p = 0; p < kS; ++p) cp16(sb + p * kPlaneB + b_swz(row, ch), src + p * g.plane_b, bytes);
           }
         }
         cp_arrive(&sm->bar_full[stg]);
@@ -817,9 +822,10 @@ bool mixed_tc_eligible(const DevMatrix* A, const DevMatrix* B) {
 // leaving C untouched, when a tile exceeds the kernel's limits (inner atoms
 // or rows); the caller then uses the mma.sync path.
 int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const MixedPlanes& mp, double* c_nrm,
-                         bool* ran, cudaEvent_t ev_prepared) {
+                         bool* ran, cudaEvent_t ev_prepared, double* tensor_ops) {
   using namespace tc;
   *ran = false;
+  *tensor_ops = 0.0;
   if (C->nnz == 0) { *ran = true; return LAMB_GPU_OK; }
   // ---- clusters (host, from the row processing order) ----
   if ((int)A->h_order.size() != A->n_rows) return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "mixed: row order missing");
@@ -917,7 +923,12 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
     std::vector<int32_t> h(n_tiles);
     LAMB_CUDA(ctx, cudaMemcpyAsync(h.data(), krows, sizeof(int32_t) * (size_t)n_tiles, cudaMemcpyDeviceToHost, ctx->stream));
     LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    for (int32_t x : h) max_rows = std::max<int64_t>(max_rows, x);
+    double steps = 0.0;
+    for (int32_t x : h) {
+      max_rows = std::max<int64_t>(max_rows, x);
+      steps += x > 0 ? (x + kK - 1) / kK : 1;
+    }
+    *tensor_ops = steps * (kS * (kS + 1) / 2) * 2.0 * kM * kN * kK;
   }
   if (max_ent > kMaxEnt || max_rows > kMaxKRows) return LAMB_GPU_OK;  // outside the kernel's limits: not run
   uint2* ent;
@@ -953,3 +964,124 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
 }
 
 }  // namespace lamb
+
+// ---- throughput probe of the tile kernel's instruction -------------------------------------
+namespace lamb {
+namespace tc {
+
+// One CTA per SM: lane 0 of warp 0 issues `iters` rounds of S(S+1)/2
+// tcgen05.mma kind::i8 (M = 128, N = n_dim, K = 32, operands from one zeroed
+// shared-memory stage, the same descriptors as the tile kernel for N = 64),
+// then waits for their completion (bounded).
+template <int N>
+__global__ void __launch_bounds__(128, 1) k_tc_probe(int iters, int* err) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ unsigned long long bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < (kStageA + N * kK * kS) / 16; i += blockDim.x)
+    reinterpret_cast<int4*>(base)[i] = make_int4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    bar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  if (warp == 0) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                 ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+      const uint32_t sa = smem_u32(base), sb = sa + kStageA;
+      // B rows of N bytes: 64-byte swizzle for N = 64, 128-byte for N >= 128 (one atom of 128 per 128 columns)
+      const uint32_t bsw = N == 64 ? 4u : 2u, bsbo = N == 64 ? 512u : 1024u, blbo = N == 64 ? 64u : 4096u;
+      const int levels = N <= 64 ? kS : 2;  // 512 tensor-memory columns hold 512 / N accumulators
+      for (int it = 0; it < iters; ++it)
+        for (int L = 0; L < kS; ++L)
+          for (int p = 0; p <= L; ++p) {
+            const uint64_t da = smem_desc(sa + p * kPlaneA, 128, 1024, 2);
+            const uint64_t db = smem_desc(sb + (L - p) * (N * kK), blbo, bsbo, bsw);
+            asm volatile(
+                "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, q;\n\t}" ::"r"(tmem + (uint32_t)(N * (L % levels))),
+                "l"(da), "l"(db), "r"(idesc), "r"(1u)
+                : "memory");
+          }
+      mma_commit(&bar);
+    }
+    __syncwarp();
+    const uint64_t t0 = now_ns();
+    while (!bar_try(&bar, 0)) {
+      if (now_ns() - t0 > 4000000000ull) {
+        atomicOr(err, 1);
+        break;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+template <int N>
+static int32_t probe_n(int device, int reps, double* tops) {
+  *tops = 0.0;
+  if (cudaSetDevice(device) != cudaSuccess) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const size_t smem = (size_t)kStageA + (size_t)N * kK * kS + 1024;
+  if (cudaFuncSetAttribute(k_tc_probe<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
+  int* err = nullptr;
+  if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return make_status(LAMB_LEVEL_MEMORY, LAMB_TYPE_EXTERNAL_ERROR);
+  cudaMemset(err, 0, sizeof(int));
+  const int iters = 2000;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_tc_probe<N><<<sms, 128, smem>>>(10, err);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < std::max(reps, 1); ++r) {
+    cudaEventRecord(e0);
+    k_tc_probe<N><<<sms, 128, smem>>>(iters, err);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  int h_err = 0;
+  const cudaError_t ce = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(err);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ce != cudaSuccess || h_err) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
+  const double ops = 2.0 * kM * N * kK * (kS * (kS + 1) / 2) * (double)iters * sms;
+  *tops = ops / (best * 1e-3) / 1e12;
+  return LAMB_GPU_OK;
+}
+
+}  // namespace tc
+}  // namespace lamb
+
+// int8 tensor-core throughput of tcgen05.mma kind::i8, M = 128, K = 32, for
+// N = 64 (the tile kernel's shape) or N = 256 (the widest instruction).
+extern "C" int32_t lamb_probe_int8_tcgen05_tops(int32_t device, int32_t n, int32_t reps, double* tops) {
+  if (!tops) return lamb::make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  if (n == 64) return lamb::tc::probe_n<64>(device, reps, tops);
+  if (n == 256) return lamb::tc::probe_n<256>(device, reps, tops);
+  return lamb::make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+}

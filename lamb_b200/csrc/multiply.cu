@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     const double* __restrict__ b_nrm, double eps, int32_t n_words, int32_t na_max, int32_t nc_max,
     const int64_t* __restrict__ c_row_p, const int64_t* __restrict__ s_row_base, int32_t* __restrict__ c_col,
     int64_t* __restrict__ stack_p, const int64_t* __restrict__ a_offk, const int64_t* __restrict__ b_off,
-    Ent* __restrict__ ent, int2* __restrict__ ids) {
+    Ent* __restrict__ ent, int2* __restrict__ ids, const int32_t* __restrict__ rows, int write_cols) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* s_anrm = reinterpret_cast<double*>(smem_raw);
   long long* s_aoff = reinterpret_cast<long long*>(s_anrm + na_max);
@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
   int* wpre = reinterpret_cast<int*>(bm + n_words);
   int* cur = wpre + n_words;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kSymThreads / 32;
-  for (int64_t i = blockIdx.x; i < n_rows; i += gridDim.x) {
+  for (int64_t idx = blockIdx.x; idx < n_rows; idx += gridDim.x) {
+    const int64_t i = rows ? rows[idx] : idx;  // C row; s_row_base is indexed by idx
     const int64_t a0 = a_row_p[i];
     const int na = (int)(a_row_p[i + 1] - a0);
     for (int t = tid; t < na; t += kSymThreads) {
@@ -228,16 +229,18 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     block_excl_scan_smem(wpre, n_words);
     const int64_t c0 = c_row_p[i];
     const int nc = (int)(c_row_p[i + 1] - c0);
-    // C columns of the row, ascending.
-    for (int w = tid; w < n_words; w += kSymThreads) {
-      uint32_t bits = bm[w];
-      int p = wpre[w];
-      while (bits) {
-        const int b = __ffs(bits) - 1;
-        bits &= bits - 1u;
-        c_col[c0 + p++] = w * 32 + b;
+    // C columns of the row, ascending (already written when the pattern was
+    // built beforehand)
+    if (write_cols)
+      for (int w = tid; w < n_words; w += kSymThreads) {
+        uint32_t bits = bm[w];
+        int p = wpre[w];
+        while (bits) {
+          const int b = __ffs(bits) - 1;
+          bits &= bits - 1u;
+          c_col[c0 + p++] = w * 32 + b;
+        }
       }
-    }
     for (int t = tid; t < nc; t += kSymThreads) cur[t] = 0;
     __syncthreads();
     for (int a = warp; a < na; a += nw) {
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(kSymThreads) k_sym_fill(
     }
     __syncthreads();
     block_excl_scan_smem(cur, nc);
-    const int64_t sb = s_row_base[i];
+    const int64_t sb = s_row_base[idx];
     for (int t = tid; t < nc; t += kSymThreads) stack_p[c0 + t] = sb + cur[t];
     __syncthreads();
     // Entries in k order: one A block at a time; the B row's columns are
@@ -315,7 +318,8 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   trace_mark(ctx, "operand norms");
   if (A->nnz >= (1ll << 31) || B->nnz >= (1ll << 31))
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "more than 2^31 blocks in an operand");
-  if (!want_ids && !a_offk && !out->pattern_only)
+  const bool pattern_now = out->pattern_only || out->chunked_fill;
+  if (!want_ids && !a_offk && !pattern_now)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "symbolic: no A meta");
   // C takes A's row subsets and B's column subsets.  Its data buffer is kept
   // for the new pattern when large enough (freed on every early return).
@@ -404,7 +408,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_TRY(dalloc(ctx, &out->stack_p, C->nnz + 1));
   if (want_ids)
     LAMB_TRY(dalloc(ctx, &out->ids, std::max<int64_t>(out->n_ent, 1)));
-  else if (out->pattern_only)
+  else if (pattern_now)
     out->ent = nullptr;
   else if (out->use_scratch)
     LAMB_TRY(scratch(ctx, kScrEnt, out->n_ent, &out->ent));
@@ -413,7 +417,17 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   LAMB_CUDA(ctx, cudaMemcpyAsync(out->stack_p + C->nnz, &h_srb[n_rows], sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
   trace_mark(ctx, "symbolic allocations");
   const size_t smem_fill = sym_fill_smem(std::max(n_words, 1), std::max<int64_t>(max_na, 1), max_c);
-  if (out->pattern_only && n_rows > 0 && C->nnz > 0) {
+  if (out->chunked_fill) {
+    out->h_row_ent = h_s;
+    out->fill_n_words = std::max(n_words, 1);
+    out->fill_na_max = (int32_t)std::max<int64_t>(max_na, 1);
+    out->fill_nc_max = (int32_t)max_c;
+    out->fill_eps = fill_eps;
+    out->fill_smem = smem_fill;
+    if (smem_fill > 220 * 1024)
+      return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
+  }
+  if (pattern_now && n_rows > 0 && C->nnz > 0) {
     const size_t smem_pat = sizeof(uint32_t) * 2 * (size_t)std::max(n_words, 1);
     if (smem_pat > 48 * 1024)
       LAMB_CUDA(ctx, cudaFuncSetAttribute(k_sym_pattern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pat));
@@ -425,7 +439,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
   } else if (smem_fill > 220 * 1024) {
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "C block row too long for the symbolic fill");
   }
-  if (!out->pattern_only && n_rows > 0 && C->nnz > 0) {
+  if (!pattern_now && n_rows > 0 && C->nnz > 0) {
     auto kern = want_ids ? k_sym_fill<true> : k_sym_fill<false>;
     if (smem_fill > 48 * 1024)
       LAMB_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fill));
@@ -437,7 +451,7 @@ int32_t symbolic_phase(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, doubl
     kern<<<fgrid, kSymThreads, smem_fill, ctx->stream>>>(
         n_rows, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, fill_eps, n_words, (int32_t)max_na,
         (int32_t)max_c, C->row_p, s_row_base, C->col, out->stack_p, a_offk, b_meta ? b_meta : B->off, out->ent,
-        out->ids);
+        out->ids, nullptr, 1);
     LAMB_LAUNCHED(ctx);
   }
   trace_mark(ctx, "symbolic fill");
@@ -482,19 +496,22 @@ int32_t pack_offk(Ctx* ctx, const DevMatrix* m, bool k_is_col, int64_t** offk) {
 }
 
 // ---- work list in the row processing order --------------------------------------------
+// row_end (optional, by position): end of every row's stack; given when the
+// stacks of consecutive rows in CSR order need not be adjacent (row chunks).
 __global__ void k_build_work(int32_t n_rows, const int32_t* __restrict__ order, const int64_t* __restrict__ cum,
                              const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                              const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                              const int8_t* __restrict__ col_bs, const int64_t* __restrict__ stack_p,
-                             Work* __restrict__ work, int32_t* __restrict__ work_c) {
+                             Work* __restrict__ work, int32_t* __restrict__ work_c,
+                             const int64_t* __restrict__ row_end) {
   const int lane = threadIdx.x & 31;
   for (int64_t w = global_warp(); w < n_rows; w += grid_warps()) {
     const int r = order[w];
     const long long bi = row_bs[r];
-    const int64_t c0 = row_p[r], v0 = cum[w] - c0;
-    for (int64_t c = c0 + lane; c < row_p[r + 1]; c += 32) {
+    const int64_t c0 = row_p[r], c1 = row_p[r + 1], v0 = cum[w] - c0;
+    for (int64_t c = c0 + lane; c < c1; c += 32) {
       const long long bj = col_bs[col[c]];
-      const long long n = stack_p[c + 1] - stack_p[c];
+      const long long n = ((row_end && c + 1 == c1) ? row_end[w] : stack_p[c + 1]) - stack_p[c];
       work[v0 + c] = Work{(long long)off[c] | (bi << 40) | (bj << 48), (long long)stack_p[c] | (n << 40)};
       work_c[v0 + c] = (int32_t)c;
     }
@@ -531,7 +548,8 @@ int32_t build_work(Ctx* ctx, const DevMatrix* C, const Symbolic& sym, const DevM
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, d_len, d_cum, n));
   k_build_work<<<grid_for(32ll * n, 256), 256, 0, ctx->stream>>>(n, order_src->order, d_cum, C->row_p, C->col, C->off,
-                                                            C->row_bs, C->col_bs, sym.stack_p, *work, *work_c);
+                                                            C->row_bs, C->col_bs, sym.stack_p, *work, *work_c,
+                                                            nullptr);
   LAMB_LAUNCHED(ctx);
   dfree(ctx, d_len);
   dfree(ctx, d_cum);
@@ -639,92 +657,162 @@ int32_t result_filter(Ctx* ctx, DevMatrix* C, const double* c_nrm, double eps) {
 }
 
 // ---- FP64 numeric phase in row chunks --------------------------------------------------
-// The work list (processing order) is cut at row boundaries into up to
-// kMaxChunks launches of about equal C-block count; an event after each marks
-// its rows' C data complete.  Inside a sector, C's data follow the same
-// processing order (layout_sector_major by_order), so chunk p's data in
-// sector s is one contiguous range; downloads copy a chunk as soon as its
-// event fires, overlapping the transfer with the remaining chunks.
+// Stack entries of one row chunk at most: 2^27 (2 GiB of 16-byte entries), or
+// the largest single C row's entries when that is more (a row is not split).
+constexpr int64_t kStackCapEntries = 1ll << 27;
+
+// The rows, in processing order, are cut into chunks: first into kMinChunks
+// of about equal C-block count (downloads copy a chunk as soon as it is
+// done), then wherever a chunk would hold more than the stack cap.  Per chunk
+// the stacks are filled into one reused buffer, the chunk's work items
+// built, and k_stacked launched; an event after each marks its rows' C data
+// complete.  Inside a sector, C's data follow the processing order
+// (layout_sector_major by_order), so chunk p's data in sector s is one
+// contiguous range.
 static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym,
-                              const Work* work, const int32_t* work_c, double* c_nrm) {
+                              const int64_t* a_offk, double* c_nrm) {
   const int mi = max_block(A->h_col_bs);
   const int n = C->n_rows, S = C->n_csub, R = C->n_rsub;
   const size_t n_sec = (size_t)R * S;
   C->n_chunks = 0;
   C->chunk_rng.clear();
-  const bool layout_ok = (int64_t)C->h_order.size() == n && (int64_t)sym.h_base.size() == (int64_t)n * S && n > 0;
-  const int P = (layout_ok && sym.c_nnz >= 4 * kMaxChunks) ? kMaxChunks : 1;
-  if (P == 1) {
-    LAMB_TRY(run_stacked(ctx, sym.c_nnz, work, work_c, sym.ent, A->data, B->data, C->data, c_nrm, false, false, mi));
-    if (layout_ok) {
-      C->n_chunks = 1;
-      C->chunk_rng.assign(2 * n_sec, 0);
-      for (size_t s2 = 0; s2 < n_sec; ++s2) C->chunk_rng[2 * s2 + 1] = C->sec_dlen[s2];
-      LAMB_CUDA(ctx, cudaEventRecord(ctx->chunk_ev[0], ctx->stream));
-      C->chunk_data = C->data;
-      ctx->chunk_m = C;
-    }
-    return LAMB_GPU_OK;
-  }
-  // chunk boundaries in processing positions, by cumulative C blocks
-  std::vector<int> q(P + 1, n);
-  q[0] = 0;
+  if (n == 0 || sym.c_nnz == 0) return LAMB_GPU_OK;
+  const std::vector<int32_t>& ord = A->h_order;
+  if ((int)ord.size() != n || !A->order || (int)sym.h_row_ent.size() != n)
+    return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "numeric: row order or row stacks missing");
+  const bool layout_ok = (int64_t)C->h_order.size() == n && (int64_t)sym.h_base.size() == (int64_t)n * S;
+  // ---- chunk boundaries (processing positions) ----
+  const int P0 = (layout_ok && sym.c_nnz >= 4 * kMinChunks) ? kMinChunks : 1;
+  std::vector<int> q0(P0 + 1, n);
+  q0[0] = 0;
   {
     int64_t acc = 0;
     int p = 1;
-    for (int w = 0; w < n && p < P; ++w) {
-      acc += sym.h_row_len[C->h_order[w]];
-      while (p < P && acc * P >= (int64_t)p * sym.c_nnz) q[p++] = w + 1;
+    for (int w = 0; w < n && p < P0; ++w) {
+      acc += sym.h_row_len[ord[w]];
+      while (p < P0 && acc * P0 >= (int64_t)p * sym.c_nnz) q0[p++] = w + 1;
     }
   }
-  // rows of each subset before every boundary
-  std::vector<int32_t> sub_of(n);
-  for (int a = 0; a < R; ++a)
-    for (int r = C->rsub_base[a]; r < C->rsub_base[a + 1]; ++r) sub_of[r] = a;
-  std::vector<int64_t> before((size_t)(P + 1) * R, 0);  // rows of subset a at positions < q[p]
-  {
-    std::vector<int64_t> cnt(R, 0);
-    int p = 0;
-    for (int w = 0; w <= n; ++w) {
-      while (p <= P && q[p] == w) {
-        for (int a = 0; a < R; ++a) before[(size_t)p * R + a] = cnt[a];
-        ++p;
+  int64_t cap = kStackCapEntries;
+  for (int w = 0; w < n; ++w) cap = std::max(cap, sym.h_row_ent[ord[w]]);
+  std::vector<int> q;
+  for (;;) {
+    q.assign(1, 0);
+    for (int p = 0; p < P0; ++p) {
+      int64_t ent = 0;
+      for (int w = q0[p]; w < q0[p + 1]; ++w) {
+        const int64_t re = sym.h_row_ent[ord[w]];
+        if (ent + re > cap && w > q.back()) {
+          q.push_back(w);
+          ent = 0;
+        }
+        ent += re;
       }
-      if (w < n) ++cnt[sub_of[C->h_order[w]]];
+      if (q0[p + 1] > q.back()) q.push_back(q0[p + 1]);
     }
+    if ((int)q.size() - 1 <= kMaxChunks) break;
+    cap *= 2;  // more chunks than events: larger chunks
   }
-  C->chunk_rng.assign(2 * (size_t)P * n_sec, 0);
-  for (int p = 0; p < P; ++p)
-    for (int a = 0; a < R; ++a)
-      for (int b = 0; b < S; ++b) {
-        const size_t s2 = (size_t)a * S + b;
-        const int64_t cnt_a = C->rsub_cnt[a];
-        auto at = [&](int64_t rank) -> int64_t {  // data offset in the sector before local rank `rank`
-          if (rank >= cnt_a) return C->sec_dlen[s2];
-          return sym.h_base[(size_t)C->rsub_base[a] * S + (size_t)b * cnt_a + rank] - C->sec_base[s2];
-        };
-        C->chunk_rng[2 * ((size_t)p * n_sec + s2)] = at(before[(size_t)p * R + a]);
-        C->chunk_rng[2 * ((size_t)p * n_sec + s2) + 1] = at(before[(size_t)(p + 1) * R + a]);
-      }
+  const int P = (int)q.size() - 1;
+  // entries before every position inside its chunk, and every chunk's total
+  std::vector<int64_t> rel(n), ends(n), ent_of(P, 0);
+  for (int p = 0; p < P; ++p) {
+    int64_t e = 0;
+    for (int w = q[p]; w < q[p + 1]; ++w) {
+      rel[w] = e;
+      e += sym.h_row_ent[ord[w]];
+      ends[w] = e;
+    }
+    ent_of[p] = e;
+  }
+  const int64_t max_ent = *std::max_element(ent_of.begin(), ent_of.end());
   // C blocks before every boundary (work items are in processing order)
   std::vector<int64_t> item(P + 1, 0);
-  {
-    int64_t acc = 0;
-    int p = 1;
-    for (int w = 0; w < n; ++w) {
-      acc += sym.h_row_len[C->h_order[w]];
-      while (p < P && q[p] == w + 1) item[p++] = acc;
-    }
-    item[P] = sym.c_nnz;
-  }
   for (int p = 0; p < P; ++p) {
-    LAMB_TRY(run_stacked(ctx, item[p + 1] - item[p], work + item[p], work_c + item[p], sym.ent, A->data, B->data,
+    int64_t acc = 0;
+    for (int w = q[p]; w < q[p + 1]; ++w) acc += sym.h_row_len[ord[w]];
+    item[p + 1] = item[p] + acc;
+  }
+  // ---- download ranges of every chunk in every sector ----
+  if (layout_ok) {
+    std::vector<int32_t> sub_of(n);
+    for (int a = 0; a < R; ++a)
+      for (int r = C->rsub_base[a]; r < C->rsub_base[a + 1]; ++r) sub_of[r] = a;
+    std::vector<int64_t> before((size_t)(P + 1) * R, 0);  // rows of subset a at positions < q[p]
+    {
+      std::vector<int64_t> cnt(R, 0);
+      int p = 0;
+      for (int w = 0; w <= n; ++w) {
+        while (p <= P && q[p] == w) {
+          for (int a = 0; a < R; ++a) before[(size_t)p * R + a] = cnt[a];
+          ++p;
+        }
+        if (w < n) ++cnt[sub_of[ord[w]]];
+      }
+    }
+    C->chunk_rng.assign(2 * (size_t)P * n_sec, 0);
+    for (int p = 0; p < P; ++p)
+      for (int a = 0; a < R; ++a)
+        for (int b = 0; b < S; ++b) {
+          const size_t s2 = (size_t)a * S + b;
+          const int64_t cnt_a = C->rsub_cnt[a];
+          auto at = [&](int64_t rank) -> int64_t {  // data offset in the sector before local rank `rank`
+            if (rank >= cnt_a) return C->sec_dlen[s2];
+            return sym.h_base[(size_t)C->rsub_base[a] * S + (size_t)b * cnt_a + rank] - C->sec_base[s2];
+          };
+          C->chunk_rng[2 * ((size_t)p * n_sec + s2)] = at(before[(size_t)p * R + a]);
+          C->chunk_rng[2 * ((size_t)p * n_sec + s2) + 1] = at(before[(size_t)(p + 1) * R + a]);
+        }
+  }
+  // ---- buffers ----
+  Ent* ent = nullptr;
+  Work* work = nullptr;
+  int32_t* work_c = nullptr;
+  LAMB_TRY(scratch(ctx, kScrEnt, max_ent, &ent));
+  LAMB_TRY(scratch(ctx, kScrWork, sym.c_nnz, &work));
+  LAMB_TRY(scratch(ctx, kScrWorkC, sym.c_nnz, &work_c));
+  int64_t *d_rel = nullptr, *d_end = nullptr, *d_len = nullptr, *d_cum = nullptr;
+  struct Free {
+    Ctx* ctx;
+    int64_t** p[4];
+    ~Free() { for (auto q : p) dfree(ctx, *q); }
+  } fr{ctx, {&d_rel, &d_end, &d_len, &d_cum}};
+  LAMB_TRY(dalloc(ctx, &d_rel, n));
+  LAMB_TRY(dalloc(ctx, &d_end, n));
+  LAMB_TRY(dalloc(ctx, &d_len, n));
+  LAMB_TRY(dalloc(ctx, &d_cum, n));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_rel, rel.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_end, ends.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  auto fill = k_sym_fill<false>;
+  if (sym.fill_smem > 48 * 1024)
+    LAMB_CUDA(ctx, cudaFuncSetAttribute(fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym.fill_smem));
+  int fgrid_all = 1;
+  LAMB_TRY(resident_grid(ctx, fill, sym.fill_smem, n, &fgrid_all));
+  // the chunk's work items: row lengths in processing order, their scan, the items
+  k_order_lens<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, A->order, C->row_p, d_len);
+  LAMB_LAUNCHED(ctx);
+  for (int p = 0; p < P; ++p) {
+    const int nr = q[p + 1] - q[p];
+    if (nr == 0) continue;
+    fill<<<std::min(fgrid_all, nr), kSymThreads, sym.fill_smem, ctx->stream>>>(
+        nr, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, sym.fill_eps, sym.fill_n_words, sym.fill_na_max,
+        sym.fill_nc_max, C->row_p, d_rel + q[p], C->col, sym.stack_p, a_offk, B->off, ent, nullptr, A->order + q[p],
+        0);
+    LAMB_LAUNCHED(ctx);
+    LAMB_TRY(exclusive_scan_i64(ctx, d_len + q[p], d_cum + q[p], nr));
+    k_build_work<<<grid_for(32ll * nr, 256), 256, 0, ctx->stream>>>(nr, A->order + q[p], d_cum + q[p], C->row_p, C->col,
+                                                                 C->off, C->row_bs, C->col_bs, sym.stack_p,
+                                                                 work + item[p], work_c + item[p], d_end + q[p]);
+    LAMB_LAUNCHED(ctx);
+    LAMB_TRY(run_stacked(ctx, item[p + 1] - item[p], work + item[p], work_c + item[p], ent, A->data, B->data,
                          C->data, c_nrm, false, false, mi));
     LAMB_CUDA(ctx, cudaEventRecord(ctx->chunk_ev[p], ctx->stream));
   }
-  C->n_chunks = P;
-  C->chunk_data = C->data;
-  ctx->chunk_m = C;
+  if (layout_ok) {
+    C->n_chunks = P;
+    C->chunk_data = C->data;
+    ctx->chunk_m = C;
+  }
   return LAMB_GPU_OK;
 }
 
@@ -747,6 +835,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   Work* work = nullptr;
   int32_t* work_c = nullptr;
   int slices = 0;
+  double tensor_ops = 0.0;
   int64_t dropped = 0;
   MixedPlanes mp;
   const bool mixed = (flags & LAMB_GPU_MIXED) != 0;
@@ -771,7 +860,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
       if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
       trace_mark(ctx, "symbolic (pattern)");
       bool ran = false;
-      LAMB_TRY(numeric_mixed_tc(ctx, A, B, C, mp, c_nrm, &ran, timed ? ctx->ev[1] : nullptr));
+      LAMB_TRY(numeric_mixed_tc(ctx, A, B, C, mp, c_nrm, &ran, timed ? ctx->ev[1] : nullptr, &tensor_ops));
       trace_mark(ctx, "numeric (tensor cores)");
       if (ran) {
         if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -799,17 +888,18 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym, mp.b_soff));
     } else {
       LAMB_TRY(pack_offk(ctx, A, true, &a_offk));
+      sym.chunked_fill = true;
       LAMB_TRY(symbolic_phase(ctx, A, B, C, eps, filt_p, false, a_offk, &sym));
     }
     trace_mark(ctx, "symbolic");
-    LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c, true));
+    if (mixed) LAMB_TRY(build_work(ctx, C, sym, A, &work, &work_c, true));
     LAMB_TRY(dalloc(ctx, &c_nrm, std::max<int64_t>(sym.c_nnz, 1)));
     trace_mark(ctx, "work items");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     if (mixed)
       LAMB_TRY(numeric_mixed(ctx, A, B, C, sym, work, work_c, c_nrm, mp));
     else
-      LAMB_TRY(numeric_chunks(ctx, A, B, C, sym, work, work_c, c_nrm));
+      LAMB_TRY(numeric_chunks(ctx, A, B, C, sym, a_offk, c_nrm));
     trace_mark(ctx, "numeric");
     if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     if (filt_r) LAMB_TRY(result_filter(ctx, C, c_nrm, eps));
@@ -837,6 +927,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   st.n_c_blocks_dropped = dropped;
   st.flops = sym.flops;
   st.mixed_slices = slices;
+  st.tensor_ops = tc_path ? tensor_ops : 0.0;
   st.kernel_launches = (int32_t)(ctx->launches - launches0);
   if (timed) {
     LAMB_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));

@@ -41,6 +41,13 @@ struct Symbolic {
   std::vector<int64_t> h_base;     // C data offset of every (row subset, column subset, rank) run
   bool use_scratch = false;    // set before symbolic_phase: ent lives in the context's scratch
   bool pattern_only = false;   // set before symbolic_phase: C's pattern and layout only, no stacks
+  // set before symbolic_phase: C's pattern and layout now, the stacks later
+  // one row chunk at a time (numeric_chunks); the fill's parameters are kept
+  bool chunked_fill = false;
+  std::vector<int64_t> h_row_ent;  // products per C row (host), with chunked_fill
+  int32_t fill_n_words = 0, fill_na_max = 0, fill_nc_max = 0;
+  double fill_eps = 0.0;
+  size_t fill_smem = 0;
 };
 void free_symbolic(Ctx* ctx, Symbolic& s);
 
@@ -99,7 +106,7 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
 bool mixed_tc_eligible(const DevMatrix* A, const DevMatrix* B);
 constexpr int kMixedTcSlices = 6;
 int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const MixedPlanes& mp, double* c_nrm,
-                         bool* ran, cudaEvent_t ev_prepared);
+                         bool* ran, cudaEvent_t ev_prepared, double* tensor_ops);
 void free_slices(Ctx* ctx, MixedPlanes* mp);
 int32_t pack_plane_meta(Ctx* ctx, const DevMatrix* A, const MixedPlanes& mp, int64_t** a_meta);
 int32_t numeric_mixed(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, const Symbolic& sym, const Work* work,

@@ -87,6 +87,8 @@ def lib() -> C.CDLL:
             "lamb_gpu_batch_execute": [vp, P(MultStats)],
             "lamb_gpu_batch_destroy": [vp],
             "lamb_gpu_batch_config": [vp, P(i32), P(i32), P(i32)],
+            "lamb_gpu_batch_run": [vp, u32, P(MultStats)],
+            "lamb_gpu_batch_queue_order": [vp, P(i32)],
         }
         for name, args in sig.items():
             f = getattr(L, name, None)
@@ -292,14 +294,23 @@ class Batch:
         self.ctx, self.h = ctx, h
 
     def execute(self) -> dict:
+        """Numeric phase only (graph replay)."""
         st = MultStats()
         self.ctx.check(lib().lamb_gpu_batch_execute(self.h, C.byref(st)))
         return st.as_dict()
 
+    def run_full(self) -> dict:
+        """Symbolic phase, graph-replayed numeric launch and result filter of
+        every instance (lamb_gpu_batch_run with LAMB_GPU_BATCH_FULL)."""
+        st = MultStats()
+        self.ctx.check(lib().lamb_gpu_batch_run(self.h, 1, C.byref(st)))
+        return st.as_dict()
+
     def config(self) -> dict:
-        w, c, g = C.c_int32(), C.c_int32(), C.c_int32()
+        w, c, g, o = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         self.ctx.check(lib().lamb_gpu_batch_config(self.h, C.byref(w), C.byref(c), C.byref(g)))
-        return {"warps": w.value, "cap": c.value, "grab": g.value}
+        self.ctx.check(lib().lamb_gpu_batch_queue_order(self.h, C.byref(o)))
+        return {"warps": w.value, "cap": c.value, "grab": g.value, "order": "shape" if o.value else "instance"}
 
     def destroy(self) -> None:
         if self.h:
