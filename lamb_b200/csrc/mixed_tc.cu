@@ -133,6 +133,15 @@ struct TcArgs {
   const int* ea;
   const int* eb;
   const int32_t* tblk;   // [tile][kMaxRowAtoms][kMaxColAtoms] C block id or -1
+  // per row cluster and tile row m: (atom index << 8 | element) or -1, and
+  // the row's exponent; per atom of the cluster: (block size << 16 | row offset)
+  const int32_t* rc_row;
+  const int32_t* rc_exp;
+  const int32_t* rc_ab;
+  // per column cluster and tile column n: (atom index << 16 | element << 8 |
+  // last element of the atom) or -1, and the column's exponent
+  const int32_t* cc_col;
+  const int32_t* cc_exp;
   const int64_t* c_off;
   double* c_data;
   double* c_nrm;
@@ -335,47 +344,31 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     int64_t local = 0;
     for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
       const int I = g.tiles[t].x, J = g.tiles[t].y;
-      const int r0 = g.rc_first[I], nra = g.rc_first[I + 1] - r0;
-      const int c0 = g.cc_first[J], nca = g.cc_first[J + 1] - c0;
-      // ---- tables of this tile (the MMAs of the tile run meanwhile) ----
-      if (et < kM) { sm->row_atom[et] = -1; sm->row_pe[et] = 0; sm->row_exp[et] = 0; }
-      if (et < kN) { sm->col_atom[et] = -1; sm->col_q[et] = 0; sm->col_last[et] = 0; sm->col_exp[et] = 0; }
-      if (et == 0) {
-        int o = 0;
-        for (int a = 0; a < nra; ++a) {
-          const int b = g.row_bs[g.rc_atoms[r0 + a]];
-          sm->row_b[a] = (int8_t)b;
-          sm->row_off[a] = (int16_t)o;
-          o += b;
-        }
-        sm->n_ra = nra;
-        sm->n_ca = nca;
+      const int nra = g.rc_first[I + 1] - g.rc_first[I];
+      const int nca = g.cc_first[J + 1] - g.cc_first[J];
+      // ---- tables of this tile (the MMAs of the tile run meanwhile); every
+      // load is independent of the others: one round of latency ----
+      {
+        const int info = g.rc_row[I * kM + et];
+        sm->row_atom[et] = (int16_t)(info >= 0 ? info >> 8 : -1);
+        sm->row_pe[et] = (int8_t)(info & 0xff);
+        sm->row_exp[et] = g.rc_exp[I * kM + et];
       }
-      named_sync(2, 128);
-      for (int a = et >> 5; a < nra; a += 4) {  // rows of atom a
-        const int atom = g.rc_atoms[r0 + a], b = sm->row_b[a], o = sm->row_off[a];
-        for (int pe = lane; pe < b; pe += 32) {
-          sm->row_atom[o + pe] = (int16_t)a;
-          sm->row_pe[o + pe] = (int8_t)pe;
-          sm->row_exp[o + pe] = g.ea[g.rbase[atom] + pe];
-        }
+      if (et < kN) {
+        const int ci = g.cc_col[J * kN + et];
+        sm->col_atom[et] = (int16_t)(ci >= 0 ? ci >> 16 : -1);
+        sm->col_q[et] = (int8_t)((ci >> 8) & 0xff);
+        sm->col_last[et] = (int8_t)(ci & 1);
+        sm->col_exp[et] = g.cc_exp[J * kN + et];
       }
-      if (et < 32) {
-        int o = 0;
-        for (int b = 0; b < nca; ++b) {
-          const int atom = g.cc_atoms[c0 + b], w = g.col_bs[atom];
-          for (int q = lane; q < w; q += 32) {
-            sm->col_atom[o + q] = (int16_t)b;
-            sm->col_q[o + q] = (int8_t)q;
-            sm->col_last[o + q] = q == w - 1;
-            sm->col_exp[o + q] = g.eb[g.cbase[atom] + q];
-          }
-          o += w;
-        }
+      if (et < kMaxRowAtoms) {
+        const int ab = g.rc_ab[I * kMaxRowAtoms + et];
+        sm->row_b[et] = (int8_t)(ab >> 16);
+        sm->row_off[et] = (int16_t)(ab & 0xffff);
       }
       for (int p = et; p < nra * kMaxColAtoms; p += 128) {
-        const int a = p / kMaxColAtoms, b = p % kMaxColAtoms;
-        const int32_t bid = b < nca ? g.tblk[t * (kMaxRowAtoms * kMaxColAtoms) + a * kMaxColAtoms + b] : -1;
+        const int b = p % kMaxColAtoms;
+        const int32_t bid = b < nca ? g.tblk[t * (kMaxRowAtoms * kMaxColAtoms) + p] : -1;
         sm->blk[p] = bid;
         sm->off[p] = bid >= 0 ? g.c_off[bid] : -1;
       }
@@ -435,32 +428,43 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     }
   } else {
     // ================= warp 3: entry loader (all lanes) and MMA issuer (lane 0) =================
-    // The loader runs one tile ahead of the producers: entries of tile
-    // `local` go to buffer local % 2.  The MMA issuer follows the stages.
-    // Both live in this warp; the loader work for tile local+1 is done
-    // between the MMA batches of tile local (entries are small).
+    // Entries of tile `local` go to buffer local % 2.  The next tile's
+    // entries are loaded into registers when a tile starts (the loads fly
+    // while its MMAs are issued) and written to shared memory after its
+    // second stage, so neither the first MMAs of a tile nor the producers'
+    // move to the next tile wait for a global load.
     int64_t gs = 0, local_mma = 0;
-    int64_t load_next = blockIdx.x, load_local = 0;
-    auto load_entries = [&](int64_t t, int64_t lidx) -> bool {
+    bool ok = true;
+    constexpr int kEntRegs = kMaxEnt / 32;
+    uint2 pre_x[kEntRegs];
+    int pre_n = 0;
+    auto prefetch = [&](int64_t t) {
+      pre_n = (int)g.ent_cnt[t];
+      const int64_t eb = g.ent_base[t];
+#pragma unroll
+      for (int j = 0; j < kEntRegs; ++j) {
+        const int e = lane + 32 * j;
+        pre_x[j] = e < pre_n ? g.ent[eb + e] : make_uint2(0u, 0u);
+      }
+    };
+    auto publish = [&](int64_t lidx) -> bool {
       const int buf = (int)(lidx & 1);
       if (!bar_wait(&sm->bar_ent_empty[buf], (uint32_t)(((lidx >> 1) & 1) ^ 1), sm, g.err, kErrTimeoutEnt))
         return false;
-      const int n = (int)g.ent_cnt[t];
-      const int64_t eb = g.ent_base[t];
-      if (n > kMaxEnt) { atomicOr(g.err, kErrEntries); sm->abort = 1; return false; }
+      if (pre_n > kMaxEnt) {
+        atomicOr(g.err, kErrEntries);
+        sm->abort = 1;
+        return false;
+      }
       int carry = 0;
-      for (int e0 = 0; e0 < n; e0 += 32) {
-        const int e = e0 + lane;
-        uint2 x = make_uint2(0u, 0u);
-        if (e < n) x = g.ent[eb + e];
-        const int bk = (int)(x.x >> 25);
-        int incl = bk;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += y;
-        }
-        if (e < n) {
+      for (int j = 0; j < kEntRegs; ++j) {
+        if (32 * j >= pre_n) break;
+        const int e = lane + 32 * j;
+        const uint2 x = pre_x[j];
+        const int bk = (int)(x.x >> 25);
+        const int incl = warp_incl_scan(bk, lane);
+        if (e < pre_n) {
           sm->ent_a[buf][e] = (int32_t)(x.x & kRowMask);
           sm->ent_b[buf][e] = (int32_t)x.y;
           sm->ent_pre[buf][e] = carry + incl - bk;
@@ -468,28 +472,21 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
         carry += __shfl_sync(0xffffffffu, incl, 31);
       }
       if (lane == 0) {
-        sm->ent_pre[buf][n] = carry;
-        sm->ent_n[buf] = n;
+        sm->ent_pre[buf][pre_n] = carry;
+        sm->ent_n[buf] = pre_n;
       }
       __syncwarp();
       bar_arrive(&sm->bar_ent_full[buf]);
       return true;
     };
-    bool ok = true;
-    // first tile's entries before any MMA
-    if (load_next < n_tiles) {
-      ok = load_entries(load_next, load_local);
-      load_next += gridDim.x;
-      ++load_local;
+    if ((int64_t)blockIdx.x < n_tiles) {
+      prefetch(blockIdx.x);
+      ok = publish(0);
     }
     for (int64_t t = blockIdx.x; ok && t < n_tiles && !sm->abort; t += gridDim.x, ++local_mma) {
-      // the next tile's entries (the producers are on this tile now)
-      if (load_next < n_tiles) {
-        ok = load_entries(load_next, load_local);
-        load_next += gridDim.x;
-        ++load_local;
-        if (!ok) break;
-      }
+      const bool has_next = t + gridDim.x < n_tiles;
+      if (has_next) prefetch(t + gridDim.x);
+      bool published = !has_next;
       const int K = g.krows[t];
       const int nst = K > 0 ? (K + kK - 1) / kK : 1;
       // tensor memory is free once the epilogue has read the previous tile
@@ -515,6 +512,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
           mma_commit(&sm->bar_empty[stg]);
         }
         __syncwarp();
+        if (!published && (s == 1 || s == nst - 1)) {
+          published = true;
+          if (!(ok = publish(local_mma + 1))) break;
+        }
       }
       if (!ok) break;
       if (lane == 0) mma_commit(&sm->bar_tmem_full);
@@ -747,6 +748,13 @@ __global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int
   }
 }
 
+// Exponent of every tile row / column of every cluster (0 for padding).
+__global__ void k_tc_cluster_exp(int64_t n, const int64_t* __restrict__ elem, const int* __restrict__ e,
+                                 int32_t* __restrict__ out) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x)
+    out[x] = elem[x] >= 0 ? e[elem[x]] : 0;
+}
+
 // ---- host ----------------------------------------------------------------------------------
 struct Clusters {
   int32_t n = 0;
@@ -843,6 +851,41 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_TRY(m.up(rc.first, &d_rcf)); LAMB_TRY(m.up(rc.atoms, &d_rca));
   LAMB_TRY(m.up(cc.of, &d_ccl)); LAMB_TRY(m.up(cc.idx, &d_catom)); LAMB_TRY(m.up(cc.off, &d_coff));
   LAMB_TRY(m.up(cc.first, &d_ccf)); LAMB_TRY(m.up(cc.atoms, &d_cca));
+  // per-cluster tables of the epilogue: row / column descriptors and exponents
+  std::vector<int32_t> h_rc_row((size_t)rc.n * kM, -1), h_rc_ab((size_t)rc.n * kMaxRowAtoms, 0);
+  std::vector<int32_t> h_cc_col((size_t)cc.n * kN, -1);
+  std::vector<int64_t> h_rc_elem((size_t)rc.n * kM, -1), h_cc_elem((size_t)cc.n * kN, -1);
+  {
+    std::vector<int64_t> rb(A->n_rows + 1, 0), cb(B->n_cols + 1, 0);
+    for (int i = 0; i < A->n_rows; ++i) rb[i + 1] = rb[i] + A->h_row_bs[i];
+    for (int j = 0; j < B->n_cols; ++j) cb[j + 1] = cb[j] + B->h_col_bs[j];
+    for (int I = 0; I < rc.n; ++I)
+      for (int a = 0; a < rc.first[I + 1] - rc.first[I]; ++a) {
+        const int atom = rc.atoms[rc.first[I] + a], b = A->h_row_bs[atom], o = rc.off[atom];
+        h_rc_ab[(size_t)I * kMaxRowAtoms + a] = (b << 16) | o;
+        for (int pe = 0; pe < b; ++pe) {
+          h_rc_row[(size_t)I * kM + o + pe] = (a << 8) | pe;
+          h_rc_elem[(size_t)I * kM + o + pe] = rb[atom] + pe;
+        }
+      }
+    for (int J = 0; J < cc.n; ++J)
+      for (int b = 0; b < cc.first[J + 1] - cc.first[J]; ++b) {
+        const int atom = cc.atoms[cc.first[J] + b], w = B->h_col_bs[atom], o = cc.off[atom];
+        for (int q = 0; q < w; ++q) {
+          h_cc_col[(size_t)J * kN + o + q] = (b << 16) | (q << 8) | (q == w - 1 ? 1 : 0);
+          h_cc_elem[(size_t)J * kN + o + q] = cb[atom] + q;
+        }
+      }
+  }
+  int32_t *d_rc_row, *d_rc_ab, *d_cc_col, *d_rc_exp, *d_cc_exp;
+  int64_t *d_rc_elem, *d_cc_elem;
+  LAMB_TRY(m.up(h_rc_row, &d_rc_row)); LAMB_TRY(m.up(h_rc_ab, &d_rc_ab)); LAMB_TRY(m.up(h_cc_col, &d_cc_col));
+  LAMB_TRY(m.up(h_rc_elem, &d_rc_elem)); LAMB_TRY(m.up(h_cc_elem, &d_cc_elem));
+  LAMB_TRY(m.alloc(&d_rc_exp, (int64_t)rc.n * kM)); LAMB_TRY(m.alloc(&d_cc_exp, (int64_t)cc.n * kN));
+  k_tc_cluster_exp<<<grid_for((int64_t)rc.n * kM), 256, 0, ctx->stream>>>((int64_t)rc.n * kM, d_rc_elem, mp.ea, d_rc_exp);
+  LAMB_LAUNCHED(ctx);
+  k_tc_cluster_exp<<<grid_for((int64_t)cc.n * kN), 256, 0, ctx->stream>>>((int64_t)cc.n * kN, d_cc_elem, mp.eb, d_cc_exp);
+  LAMB_LAUNCHED(ctx);
   // ---- inner-atom bitmaps and panel row offsets ----
   uint32_t *bma, *bmb;
   int32_t *wra, *wrb;
@@ -947,6 +990,7 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   g.rc_first = d_rcf; g.rc_atoms = d_rca; g.cc_first = d_ccf; g.cc_atoms = d_cca;
   g.row_bs = C->row_bs; g.col_bs = C->col_bs; g.rbase = mp.rbase; g.cbase = mp.cbase; g.ea = mp.ea; g.eb = mp.eb;
   g.tblk = tblk; g.c_off = C->off; g.c_data = C->data; g.c_nrm = c_nrm; g.err = d_err;
+  g.rc_row = d_rc_row; g.rc_exp = d_rc_exp; g.rc_ab = d_rc_ab; g.cc_col = d_cc_col; g.cc_exp = d_cc_exp;
   LAMB_CUDA(ctx, cudaFuncSetAttribute(k_tc_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

@@ -93,19 +93,29 @@ def test_masked_adjoint_matches_dense(gpu_ctx):
 
 def test_mcweeny_mixed_early_steps_match_fp64(gpu_ctx):
     """Purification with int8-slice products in the early steps and an FP64
-    tail reaches the all-FP64 density matrix and band energy Tr(P.H)."""
+    tail reaches the all-FP64 density matrix and band energy Tr(P.H).
+
+    Both runs filter products and C blocks at eps = 1e-10, but not the same
+    ones: the tensor-core mixed products keep every product (also those below
+    eps), the FP64 products skip them, so the two truncated iterations end a
+    few 1e-9 apart.  Against an unfiltered FP64 run (eps = 0) the mixed run
+    is as close as the filtered FP64 run."""
     g = WaterGeometry(48, None, 5.5, seed=6)
     h = gapped_hamiltonian(g, 3)
     dh = gpu_ctx.upload(h)
-    p64, pmx = gpu_ctx.create_like(dh), gpu_ctx.create_like(dh)
+    p64, pmx, pex = gpu_ctx.create_like(dh), gpu_ctx.create_like(dh), gpu_ctx.create_like(dh)
     r64 = gpu_ctx.purify(dh, p64, mu=0.0, steps=30, fp64_tail=30, eps=1e-10)
     rmx = gpu_ctx.purify(dh, pmx, mu=0.0, steps=30, fp64_tail=5, eps=1e-10)
+    gpu_ctx.purify(dh, pex, mu=0.0, steps=30, fp64_tail=30, eps=0.0)
     assert rmx["steps_mixed"] == 25 and r64["steps_mixed"] == 0
-    rel = gpu_ctx.diff_frobenius(pmx, p64) / gpu_ctx.frobenius(p64)
+    nrm = gpu_ctx.frobenius(pex)
+    rel = gpu_ctx.diff_frobenius(pmx, p64) / nrm
+    rel_mx, rel_64 = gpu_ctx.diff_frobenius(pmx, pex) / nrm, gpu_ctx.diff_frobenius(p64, pex) / nrm
     e64, emx = gpu_ctx.trace_product(p64, dh), gpu_ctx.trace_product(pmx, dh)
-    assert rel < 1e-9
+    assert rel < 5e-9
+    assert rel_mx <= max(2 * rel_64, 1e-10), (rel_mx, rel_64)
     assert abs(emx - e64) <= 1e-9 * abs(e64)
     assert abs(rmx["trace"] - r64["trace"]) < 1e-8
     assert rmx["idempotency"] < 1e-8
-    for m in (pmx, p64, dh):
+    for m in (pex, pmx, p64, dh):
         m.destroy()

@@ -50,7 +50,7 @@ def test_batch_full_run_with_filters(gpu_ctx):
     and result filter of every instance, O 23 and O 13 instances, both
     filters active; every C against the oracle with the same filters, twice
     (the second full run refreshes the queue in place and replays)."""
-    eps = 2e-3
+    eps = 3e-2  # drops products and C blocks in these boxes
     wls = batch_instances(n=4, seed=7, mol_range=(16, 60), cut_range=(4.5, 7.0))
     assert {wl.blk_o for wl in wls} == {13, 23}
     hosts, devs = [], []

@@ -362,7 +362,7 @@ def test_mixed_tensor_core_keeps_filtered_pattern(gpu_ctx):
     against the unfiltered product on that pattern."""
     g = WaterGeometry(48, None, 6.0, seed=8)
     a, b = g.matrix(1), g.matrix(2)
-    eps = 1e-3
+    eps = 1e-2  # about 13 % of the products fall below it
     c_ref, st_ref = oracle.multiply(a, b, eps, oracle.NO_RESULT_FILTER)
     assert st_ref["n_products_skipped"] > 0
     c, st = _gpu_mult(gpu_ctx, a, b, eps, gpu.MIXED | gpu.NO_RESULT_FILTER)
