@@ -39,8 +39,14 @@
 //   warp 3     loads each tile's inner-atom list one tile ahead, allocates
 //              the tensor memory (6 levels x 64 columns in 512) and from one
 //              lane issues S(S+1)/2 MMAs (M=128, N=64, K=32) per stage;
-//   warps 4-7  epilogue: tensor memory -> registers, FP64 recombination,
-//              scaling, scatter into C's blocks and their norms.
+//   warps 4-7  epilogue: tensor memory -> registers (the six levels of a
+//              column recombined exactly in two int64 sums, then FP64),
+//              scaling into a staging tile in shared memory, per-row
+//              partial sums of squares per column atom; then every C block
+//              of the tile copied out in its storage order (contiguous
+//              stores, one warp a block) and its norm summed from the row
+//              partials.  The tile's block list (built before the kernel)
+//              and exponents are loaded one tile ahead into registers.
 // Every wait on an mbarrier is bounded (2 s of %globaltimer); on a timeout
 // the kernel records an error code, every role stops, and the host returns
 // an error status.
@@ -58,7 +64,7 @@ namespace tc {
 
 constexpr int kS = 6;                 // digits per operand
 constexpr int kM = 128, kN = 64, kK = 32;
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kPlaneA = kK * kM;      // bytes of one digit plane of one stage (A)
 constexpr int kPlaneB = kK * kN;
 constexpr int kStageA = kS * kPlaneA;
@@ -67,6 +73,15 @@ constexpr int kStageBytes = kStageA + kStageB;  // 36,864: a multiple of 1,024
 constexpr int kMaxEnt = 1024;         // inner atoms of one tile
 constexpr int kMaxRowAtoms = 32;      // atoms of one row cluster
 constexpr int kMaxColAtoms = 16;      // atoms of one column cluster
+constexpr int kMaxBlocks = kMaxRowAtoms * kMaxColAtoms;  // C blocks of one tile
+constexpr int kPartStride = kMaxColAtoms + 1;  // padded: the rows of a warp hit distinct banks
+// An integer x with |x| < 2^51 added to the bit pattern of 2^52 + 2^51 gives
+// the double 2^52 + 2^51 + x exactly; subtracting that constant leaves x.
+constexpr long long kBias = 0x4338000000000000LL;
+constexpr double kBiasD = 6755399441055744.0;
+// Exponents up to this size scale by multiplying with exact powers of two
+// (no intermediate can under- or overflow); larger ones go through ldexp.
+constexpr int kExactExp = 500;
 constexpr int kTileThreads = 256;
 constexpr int kProducers = 96;
 constexpr int kTmemCols = 512;
@@ -84,25 +99,23 @@ enum : int { kErrTimeoutFull = 1, kErrTimeoutEmpty = 2, kErrTimeoutTmemFull = 4,
 
 // ---- shared-memory layout of the tile kernel --------------------------------------------
 struct __align__(16) TileSmem {
+  // the tile's scaled FP64 values: element (m, n) at m * kN + (n ^ (m % 16))
+  double stg[kM * kN];
+  // sum of squares of row m over the columns of column atom b, at m * kPartStride + b
+  double part[kM * kPartStride];
   // entries of two tiles (the loader fills one while the producers use the other)
   int32_t ent_a[2][kMaxEnt];
   int32_t ent_b[2][kMaxEnt];
-  int32_t ent_pre[2][kMaxEnt + 1];
+  uint16_t ent_pre[2][kMaxEnt + 8];  // first K row of every entry (K rows < 2^16)
   int32_t ent_n[2];
   // epilogue tables of the current tile
-  int32_t blk[kMaxRowAtoms * kMaxColAtoms];
-  long long off[kMaxRowAtoms * kMaxColAtoms];
-  double part[kM][kMaxColAtoms];
-  int16_t row_atom[kM];   // atom index within the row cluster, -1 for padding rows
-  int8_t row_pe[kM];
-  int32_t row_exp[kM];
-  int8_t row_b[kMaxRowAtoms];
-  int16_t row_off[kMaxRowAtoms];
-  int16_t col_atom[kN];
-  int8_t col_q[kN];
-  int8_t col_last[kN];
+  long long blk_off[kMaxBlocks];  // data offset of each C block of the tile
+  int32_t blk_id[kMaxBlocks];     // its index in C
+  int32_t blk_geom[kMaxBlocks];   // its first tile row, first tile column, sizes, column atom
+  double col_scale[kN];           // 2^exponent of every tile column (when not wide)
   int32_t col_exp[kN];
-  int32_t n_ra, n_ca;
+  int32_t col_info[kN];           // column atom << 1 | last column of the atom (0 for padding)
+  int32_t n_blk;
   unsigned long long bar_full[kStages], bar_empty[kStages];
   unsigned long long bar_tmem_full, bar_tmem_empty, bar_ent_full[2], bar_ent_empty[2], bar_done;
   uint32_t tmem_base;
@@ -110,6 +123,8 @@ struct __align__(16) TileSmem {
 };
 
 constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + sizeof(TileSmem) + 1024;  // + alignment slack
+static_assert(kSmemBytes <= 232448, "tile kernel exceeds the shared memory of one CTA");
+static_assert(kMaxKRows < 65536, "entry starts are stored as 16-bit K rows");
 
 struct TcArgs {
   const int2* tiles;
@@ -132,17 +147,16 @@ struct TcArgs {
   const int64_t* cbase;  // first element column of every B column atom
   const int* ea;
   const int* eb;
-  const int32_t* tblk;   // [tile][kMaxRowAtoms][kMaxColAtoms] C block id or -1
-  // per row cluster and tile row m: (atom index << 8 | element) or -1, and
-  // the row's exponent; per atom of the cluster: (block size << 16 | row offset)
-  const int32_t* rc_row;
+  // C blocks of every tile: tile t owns blist[lbase[t] .. lbase[t + 1]),
+  // each (C block index, geometry, data offset low, high word)
+  const int4* blist;
+  const int64_t* lbase;
+  // per row cluster and tile row m the row's exponent (0 for padding)
   const int32_t* rc_exp;
-  const int32_t* rc_ab;
-  // per column cluster and tile column n: (atom index << 16 | element << 8 |
-  // last element of the atom) or -1, and the column's exponent
-  const int32_t* cc_col;
+  // per column cluster and tile column n: the column's exponent, and
+  // (column atom << 1 | last column of the atom) or 0 for padding
   const int32_t* cc_exp;
-  const int64_t* c_off;
+  const int32_t* cc_col;
   double* c_data;
   double* c_nrm;
   int* err;
@@ -152,6 +166,11 @@ struct TcArgs {
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
+// x * 2^e for any e, out of line: the scatter loop is unrolled 64 times and
+// only exponents beyond kExactExp (not met in practice) take this path.
+__device__ __noinline__ double scale_wide(double x, int e) { return ldexp(x, e); }
+// 2^e for -1022 <= e <= 1023, exactly.
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 __device__ __forceinline__ uint64_t now_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -172,20 +191,31 @@ __device__ __forceinline__ bool bar_try(unsigned long long* b, uint32_t parity) 
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: a waiting thread sleeps in hardware
+// (issuing nothing) until the phase completes or about `ns` nanoseconds pass.
+__device__ __forceinline__ bool bar_try_sleep(unsigned long long* b, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 // Waits until the phase with the given parity has completed; gives up after
-// 2 s (or when another role aborted), recording `code`.
+// 2 s (or when another role aborted), recording `code`.  The waiting thread
+// sleeps between checks, leaving the issue slots to the other warps of its
+// SM sub-partition.
 __device__ __forceinline__ bool bar_wait(unsigned long long* b, uint32_t parity, TileSmem* sm, int* err, int code) {
   if (bar_try(b, parity)) return true;
   const uint64_t t0 = now_ns();
-  for (uint32_t it = 1;; ++it) {
-    if (bar_try(b, parity)) return true;
-    if ((it & 255) == 0) {
-      if (*(volatile int*)&sm->abort) return false;
-      if (now_ns() - t0 > 2000000000ull) {
-        atomicOr(err, code);
-        *(volatile int*)&sm->abort = 1;
-        return false;
-      }
+  for (;;) {
+    if (bar_try_sleep(b, parity, 200000u)) return true;
+    if (*(volatile int*)&sm->abort) return false;
+    if (now_ns() - t0 > 2000000000ull) {
+      atomicOr(err, code);
+      *(volatile int*)&sm->abort = 1;
+      return false;
     }
   }
 }
@@ -199,6 +229,16 @@ __device__ __forceinline__ void cp_arrive(unsigned long long* b) {
 }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+// Named barrier that also returns the OR of every participant's predicate.
+__device__ __forceinline__ bool named_sync_or(int id, int n, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -214,15 +254,17 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;
 }
 // Instruction descriptor: kind::i8, signed A and B, int32 accumulator, both
-// operands MN-major, N = 64, M = 128.
-constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(kN >> 3) << 17) |
-                            ((uint32_t)(kM >> 4) << 24);
+// operands MN-major, M = 128, the given N (a multiple of 16 up to 256).
+constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kM >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
       : "memory");
 }
 __device__ __forceinline__ void mma_commit(unsigned long long* b) {
@@ -238,6 +280,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
         "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
         "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -298,29 +345,35 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       const int n = sm->ent_n[buf];
       const int K = g.krows[t];
       const int nst = K > 0 ? (K + kK - 1) / kK : 1;
-      const int32_t* pre = sm->ent_pre[buf];
+      const uint16_t* pre = sm->ent_pre[buf];
       for (int s = 0; s < nst; ++s, ++gs) {
         const int stg = (int)(gs % kStages);
         if (!bar_wait(&sm->bar_empty[stg], (uint32_t)(((gs / kStages) & 1) ^ 1), sm, g.err, kErrTimeoutEmpty)) break;
         const uint32_t sa = smem_u32(stages + (size_t)stg * kStageBytes);
         const uint32_t sb = sa + kStageA;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int u = pt + kProducers * i;
-          const bool is_a = u < 256;
-          const int row = is_a ? (u >> 3) : ((u - 256) >> 2);
-          const int ch = is_a ? (u & 7) : ((u - 256) & 3);
-          const int kk = s * kK + row;
-          const bool valid = kk < K;
-          int64_t prow = 0;
-          if (valid) {
+        // lane r of every producer warp finds the panel rows of the stage's
+        // inner row r (one search per lane); the units take them by shuffle
+        int my_a = 0, my_b = 0;
+        {
+          const int kk = s * kK + lane;
+          if (kk < K) {
             int lo = 0, hi = n - 1;  // last entry e with pre[e] <= kk
             while (lo < hi) {
               const int mid = (lo + hi + 1) >> 1;
               if (pre[mid] <= kk) lo = mid; else hi = mid - 1;
             }
-            prow = (is_a ? sm->ent_a[buf][lo] : sm->ent_b[buf][lo]) + (kk - pre[lo]);
+            my_a = sm->ent_a[buf][lo] + (kk - pre[lo]);
+            my_b = sm->ent_b[buf][lo] + (kk - pre[lo]);
           }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int u = pt + kProducers * i;
+          const bool is_a = u < 256;  // uniform over the warp
+          const int row = is_a ? (u >> 3) : ((u - 256) >> 2);
+          const int ch = is_a ? (u & 7) : ((u - 256) & 3);
+          const bool valid = s * kK + row < K;
+          const int64_t prow = __shfl_sync(0xffffffffu, is_a ? my_a : my_b, row);
           const uint32_t bytes = valid ? 16u : 0u;
           if (is_a) {
             const int8_t* src = g.pan_a + prow * 128 + 16 * ch;
@@ -341,98 +394,187 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     // ================= epilogue =================
     const int et = tid - 128;       // 0..127: tile row m
     const int ew = warp - 4;        // tensor-memory lane quarter
-    int64_t local = 0;
-    for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
-      const int I = g.tiles[t].x, J = g.tiles[t].y;
-      const int nra = g.rc_first[I + 1] - g.rc_first[I];
-      const int nca = g.cc_first[J + 1] - g.cc_first[J];
-      // ---- tables of this tile (the MMAs of the tile run meanwhile); every
-      // load is independent of the others: one round of latency ----
-      {
-        const int info = g.rc_row[I * kM + et];
-        sm->row_atom[et] = (int16_t)(info >= 0 ? info >> 8 : -1);
-        sm->row_pe[et] = (int8_t)(info & 0xff);
-        sm->row_exp[et] = g.rc_exp[I * kM + et];
-      }
+    // Tables of the next tile, loaded into registers while the current tile
+    // is copied out: its row exponent (this thread's row), column exponent
+    // and column info (threads < kN), block count and up to kMaxBlocks / 128
+    // block-list entries per thread.  The list bounds of the tile after next
+    // are loaded one tile earlier still, so no load waits on another.
+    constexpr int kBlkRegs = kMaxBlocks / 128;
+    int nx_er = 0, nx_ec = 0, nx_ci = 0, nx_nb = 0;
+    int4 nx_b[kBlkRegs];
+    int64_t lb_lo = 0, lb_hi = 0;  // list bounds of the tile being prefetched
+    int2 lb_tile = make_int2(0, 0);  // and its clusters
+    auto bounds = [&](int64_t t) {
+      lb_lo = t < n_tiles ? g.lbase[t] : 0;
+      lb_hi = t < n_tiles ? g.lbase[t + 1] : 0;
+      lb_tile = t < n_tiles ? g.tiles[t] : make_int2(0, 0);
+    };
+    auto prefetch = [&]() {
+      const int I = lb_tile.x, J = lb_tile.y;
+      nx_er = g.rc_exp[(int64_t)I * kM + et];
       if (et < kN) {
-        const int ci = g.cc_col[J * kN + et];
-        sm->col_atom[et] = (int16_t)(ci >= 0 ? ci >> 16 : -1);
-        sm->col_q[et] = (int8_t)((ci >> 8) & 0xff);
-        sm->col_last[et] = (int8_t)(ci & 1);
-        sm->col_exp[et] = g.cc_exp[J * kN + et];
+        nx_ec = g.cc_exp[(int64_t)J * kN + et];
+        nx_ci = g.cc_col[(int64_t)J * kN + et];
       }
-      if (et < kMaxRowAtoms) {
-        const int ab = g.rc_ab[I * kMaxRowAtoms + et];
-        sm->row_b[et] = (int8_t)(ab >> 16);
-        sm->row_off[et] = (int16_t)(ab & 0xffff);
+      nx_nb = (int)(lb_hi - lb_lo);
+#pragma unroll
+      for (int j = 0; j < kBlkRegs; ++j) {
+        const int k = et + 128 * j;
+        nx_b[j] = k < nx_nb ? g.blist[lb_lo + k] : make_int4(0, 0, 0, 0);
       }
-      for (int p = et; p < nra * kMaxColAtoms; p += 128) {
-        const int b = p % kMaxColAtoms;
-        const int32_t bid = b < nca ? g.tblk[t * (kMaxRowAtoms * kMaxColAtoms) + p] : -1;
-        sm->blk[p] = bid;
-        sm->off[p] = bid >= 0 ? g.c_off[bid] : -1;
+    };
+    // Writes the prefetched tables to shared memory; returns whether some
+    // exponent of the tile lies beyond kExactExp (the same for every thread).
+    auto publish = [&]() -> bool {
+      if (et < kN) {
+        sm->col_exp[et] = nx_ec;
+        sm->col_scale[et] = pow2(nx_ec < -kExactExp || nx_ec > kExactExp ? 0 : nx_ec);
+        sm->col_info[et] = nx_ci;
       }
-      named_sync(2, 128);
-      // ---- accumulators ----
-      if (!bar_wait(&sm->bar_tmem_full, (uint32_t)(local & 1), sm, g.err, kErrTimeoutTmemFull)) break;
-      tc_fence_after();
-      double acc[kN];
 #pragma unroll
-      for (int n = 0; n < kN; ++n) acc[n] = 0.0;
-#pragma unroll
-      for (int L = kS - 1; L >= 0; --L) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          int v[32];
-          tmem_ld32(tmem + ((uint32_t)(32 * ew) << 16) + (uint32_t)(64 * L + 32 * h), v);
-          tmem_wait_ld();
-#pragma unroll
-          for (int c = 0; c < 32; ++c) acc[32 * h + c] = __fma_rn((double)v[c], kLevelW[L], acc[32 * h + c]);
+      for (int j = 0; j < kBlkRegs; ++j) {
+        const int k = et + 128 * j;
+        if (k < nx_nb) {
+          sm->blk_id[k] = nx_b[j].x;
+          sm->blk_geom[k] = nx_b[j].y;
+          sm->blk_off[k] = (long long)(((uint64_t)(uint32_t)nx_b[j].w << 32) | (uint32_t)nx_b[j].z);
         }
       }
-      tc_fence_before();
-      bar_arrive(&sm->bar_tmem_empty);
-      // ---- scaling and scatter ----
-      const int a = sm->row_atom[et];
-      double run = 0.0;
-      if (a >= 0) {
-        const int pe = sm->row_pe[et], bi = sm->row_b[a], er = sm->row_exp[et];
+      if (et == 0) sm->n_blk = nx_nb;
+      const bool w = nx_er < -kExactExp || nx_er > kExactExp || (et < kN && (nx_ec < -kExactExp || nx_ec > kExactExp));
+      return named_sync_or(2, 128, w);
+    };
+    int64_t local = 0;
+    bool wide = false;
+    int er = 0;
+    if ((int64_t)blockIdx.x < n_tiles) {
+      bounds(blockIdx.x);
+      prefetch();
+      bounds(blockIdx.x + (int64_t)gridDim.x);
+      er = nx_er;
+      wide = publish();
+    }
+    for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
+      const bool has_next = t + gridDim.x < n_tiles;
+      // ---- accumulators: tensor memory -> staging tile, 8 columns a round
+      // (a rolled loop: the epilogue's code stays small next to the other
+      // roles' in the instruction cache).  Per column the six level sums v_L
+      // recombine as (v0 254^2 + v1 254 + v2) w_2 + (v3 254^2 + v4 254 + v5) w_5
+      // with w_L = 1 / (127^2 254^L): both brackets are exact in int64
+      // (|v_L| < 2^31), below 2^51 in magnitude, and convert exactly to FP64
+      // by the 2^52 + 2^51 bias.  The row's power of two is folded into w_2
+      // and w_5 (exact: |er| <= kExactExp).  Tensor memory is released as
+      // soon as the tile is staged: the next tile's MMAs wait for nothing else. ----
+      if (!bar_wait(&sm->bar_tmem_full, (uint32_t)(local & 1), sm, g.err, kErrTimeoutTmemFull)) break;
+      tc_fence_after();
+      double* row = sm->stg + et * kN;
+      const int sw = et & 15;
+      {
+        const double rs = wide ? 1.0 : pow2(er);
+        const double w2 = kLevelW[2] * rs, w5 = kLevelW[5] * rs;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * ew) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < kN; c0 += 8) {
+          int v[kS][8];
 #pragma unroll
-        for (int n = 0; n < kN; ++n) {
-          const int b = sm->col_atom[n];
-          if (b >= 0) {
-            const long long o = sm->off[a * kMaxColAtoms + b];
-            if (o >= 0) {
-              const double val = ldexp(acc[n], er + sm->col_exp[n]);
-              g.c_data[o + (int64_t)sm->col_q[n] * bi + pe] = val;
-              run = __fma_rn(val, val, run);
+          for (int L = 0; L < kS; ++L) tmem_ld8(lane_base + (uint32_t)(64 * L + c0), v[L]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const long long hi = kBias + (long long)v[0][c] * 64516 + (long long)v[1][c] * 254 + v[2][c];
+            const long long lo = kBias + (long long)v[3][c] * 64516 + (long long)v[4][c] * 254 + v[5][c];
+            const double hd = __longlong_as_double(hi) - kBiasD, ld = __longlong_as_double(lo) - kBiasD;
+            row[(c0 + c) ^ sw] = __fma_rn(hd, w2, ld * w5);
+          }
+        }
+        tc_fence_before();
+        bar_arrive(&sm->bar_tmem_empty);  // the MMAs of the next tile may start
+      }
+      if (has_next) {
+        prefetch();
+        bounds(t + 2 * (int64_t)gridDim.x);
+      }
+      // ---- column scaling in place and the row partials of the sums of
+      // squares (column order within each column atom) ----
+      {
+        double* part = sm->part + et * kPartStride;
+        double run = 0.0;
+        if (!wide) {
+#pragma unroll 1
+          for (int n = 0; n < kN; n += 4) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              const double y = row[(n + c) ^ sw] * sm->col_scale[n + c];
+              row[(n + c) ^ sw] = y;
+              run = __fma_rn(y, y, run);
+              const int ci = sm->col_info[n + c];
+              if (ci & 1) {
+                part[ci >> 1] = run;
+                run = 0.0;
+              }
             }
-            if (sm->col_last[n]) {
-              sm->part[et][b] = run;
+          }
+        } else {  // rare: exponents beyond kExactExp, scaled out of line
+          for (int n = 0; n < kN; ++n) {
+            const double y = scale_wide(row[n ^ sw], er + sm->col_exp[n]);
+            row[n ^ sw] = y;
+            run = __fma_rn(y, y, run);
+            const int ci = sm->col_info[n];
+            if (ci & 1) {
+              part[ci >> 1] = run;
               run = 0.0;
             }
           }
         }
       }
       named_sync(2, 128);
-      // ---- block norms in a fixed order (rows of the block ascending) ----
-      for (int p = et; p < nra * kMaxColAtoms; p += 128) {
-        const int32_t bid = sm->blk[p];
-        if (bid < 0) continue;
-        const int aa = p / kMaxColAtoms, b = p % kMaxColAtoms;
-        double s = 0.0;
-        for (int pe = 0; pe < sm->row_b[aa]; ++pe) s += sm->part[sm->row_off[aa] + pe][b];
-        g.c_nrm[bid] = __dsqrt_rn(s);
+      // ---- copy-out: one warp per C block, elements in storage order
+      // (column-major: element e is (e % bi, e / bi)), contiguous stores ----
+      const int nb = sm->n_blk;
+      for (int k = ew; k < nb; k += 4) {
+        const int geo = sm->blk_geom[k];
+        const int r0 = geo & 127, c0 = (geo >> 7) & 63, bi = (geo >> 13) & 127, bj = (geo >> 20) & 127;
+        double* __restrict__ out = g.c_data + sm->blk_off[k];
+        // lane / bi and 32 / bi: the float quotient is at least 0.5 / bi away
+        // from the next integer, far more than its rounding error
+        const float rcp = __frcp_rn((float)bi);
+        int q = (int)(((float)lane + 0.5f) * rcp);
+        int pe = lane - q * bi;
+        const int step_q = (int)(32.5f * rcp), step_r = 32 - step_q * bi;
+        const int ne = bi * bj;
+#pragma unroll 4
+        for (int e = lane; e < ne; e += 32) {
+          const int mm = r0 + pe, nn = c0 + q;
+          out[e] = sm->stg[mm * kN + (nn ^ (mm & 15))];
+          pe += step_r;
+          q += step_q;
+          if (pe >= bi) {
+            pe -= bi;
+            ++q;
+          }
+        }
       }
-      named_sync(2, 128);
+      // ---- block norms: rows of the block in ascending order ----
+      for (int k = et; k < nb; k += 128) {
+        const int geo = sm->blk_geom[k];
+        const int r0 = geo & 127, bi = (geo >> 13) & 127, cb = (geo >> 27) & 15;
+        double sq = 0.0;
+        for (int pe = 0; pe < bi; ++pe) sq += sm->part[(r0 + pe) * kPartStride + cb];
+        g.c_nrm[sm->blk_id[k]] = __dsqrt_rn(sq);
+      }
+      named_sync(2, 128);  // the staging tile and the tables are free again
+      if (has_next) {
+        er = nx_er;
+        wide = publish();
+      }
     }
   } else {
     // ================= warp 3: entry loader (all lanes) and MMA issuer (lane 0) =================
     // Entries of tile `local` go to buffer local % 2.  The next tile's
-    // entries are loaded into registers when a tile starts (the loads fly
-    // while its MMAs are issued) and written to shared memory after its
-    // second stage, so neither the first MMAs of a tile nor the producers'
-    // move to the next tile wait for a global load.
+    // entries are loaded into registers when a tile starts and written to
+    // shared memory once the tile's tensor memory is free (the loads fly
+    // meanwhile), before its first MMA, so the producers can move on to the
+    // next tile as soon as they have issued this one.
     int64_t gs = 0, local_mma = 0;
     bool ok = true;
     constexpr int kEntRegs = kMaxEnt / 32;
@@ -467,12 +609,12 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
         if (e < pre_n) {
           sm->ent_a[buf][e] = (int32_t)(x.x & kRowMask);
           sm->ent_b[buf][e] = (int32_t)x.y;
-          sm->ent_pre[buf][e] = carry + incl - bk;
+          sm->ent_pre[buf][e] = (uint16_t)(carry + incl - bk);
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
       }
       if (lane == 0) {
-        sm->ent_pre[buf][pre_n] = carry;
+        sm->ent_pre[buf][pre_n] = (uint16_t)carry;
         sm->ent_n[buf] = pre_n;
       }
       __syncwarp();
@@ -492,6 +634,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       // tensor memory is free once the epilogue has read the previous tile
       if (!bar_wait(&sm->bar_tmem_empty, (uint32_t)((local_mma & 1) ^ 1), sm, g.err, kErrTimeoutTmemEmpty)) break;
       tc_fence_after();
+      if (!published) {  // the prefetch has landed meanwhile
+        published = true;
+        if (!(ok = publish(local_mma + 1))) break;
+      }
       for (int s = 0; s < nst; ++s, ++gs) {
         const int stg = (int)(gs % kStages);
         if (!bar_wait(&sm->bar_full[stg], (uint32_t)((gs / kStages) & 1), sm, g.err, kErrTimeoutFull)) { ok = false; break; }
@@ -500,22 +646,26 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
           fence_async_smem();
           const uint32_t sa = smem_u32(stages + (size_t)stg * kStageBytes);
           const uint32_t sb = sa + kStageA;
+          // A plane p times B planes q0 .. q0 + nq - 1 in one MMA of N = 64 nq:
+          // the B planes lie kPlaneB apart, which the descriptor's leading
+          // byte offset steps through as consecutive 64-column chunks of N,
+          // and their products land on consecutive level accumulators
+          // 64 (p + q) of tensor memory.  Nine MMAs per stage cover the 21
+          // pairs p + q < 6 (N <= 256 per instruction), reading A nine times
+          // instead of 21.
 #pragma unroll
-          for (int L = 0; L < kS; ++L)
+          for (int p = 0; p < kS; ++p) {
+            const uint64_t da = smem_desc(sa + p * kPlaneA, 128, 1024, 2);
 #pragma unroll
-            for (int p = 0; p <= L; ++p) {
-              const int q = L - p;
-              const uint64_t da = smem_desc(sa + p * kPlaneA, 128, 1024, 2);
-              const uint64_t db = smem_desc(sb + q * kPlaneB, 64, 512, 4);
-              mma_i8(tmem + (uint32_t)(64 * L), da, db, (s > 0 || p > 0) ? 1u : 0u);
+            for (int q0 = 0; q0 < kS - p; q0 += 4) {
+              const int nq = (kS - p - q0) < 4 ? (kS - p - q0) : 4;
+              const uint64_t db = smem_desc(sb + q0 * kPlaneB, kPlaneB, 512, 4);
+              mma_i8(tmem + (uint32_t)(64 * (p + q0)), da, db, idesc_i8(64 * nq), (s > 0 || p > 0) ? 1u : 0u);
             }
+          }
           mma_commit(&sm->bar_empty[stg]);
         }
         __syncwarp();
-        if (!published && (s == 1 || s == nst - 1)) {
-          published = true;
-          if (!(ok = publish(local_mma + 1))) break;
-        }
       }
       if (!ok) break;
       if (lane == 0) mma_commit(&sm->bar_tmem_full);
@@ -678,19 +828,32 @@ __global__ void k_tc_tile_list(int64_t n_map, int32_t n_cc, const int64_t* __res
     if (flag[x]) tiles[pos[x]] = make_int2((int)(x / n_cc), (int)(x % n_cc));
 }
 
-// C block ids of every tile, at [tile][row atom][column atom].
+// C blocks of every tile.  Count pass: blocks per tile.  Fill pass: one
+// list entry per block at lbase[t] + (arrival order within the tile), each
+// (block index, geometry, data offset) with geometry = first tile row |
+// first tile column << 7 | bi << 13 | bj << 20 | column atom << 27.  The
+// order within a tile only decides which warp copies which block.
+template <bool FILL>
 __global__ void k_tc_tile_blocks(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
-                                 const int32_t* __restrict__ rcl, const int32_t* __restrict__ ratom,
-                                 const int32_t* __restrict__ ccl, const int32_t* __restrict__ catom, int32_t n_cc,
-                                 const int64_t* __restrict__ pos, int32_t* __restrict__ tblk) {
+                                 const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
+                                 const int8_t* __restrict__ col_bs, const int32_t* __restrict__ rcl,
+                                 const int32_t* __restrict__ roff, const int32_t* __restrict__ ccl,
+                                 const int32_t* __restrict__ coff, const int32_t* __restrict__ catom, int32_t n_cc,
+                                 const int64_t* __restrict__ pos, int64_t* __restrict__ cnt,
+                                 const int64_t* __restrict__ lbase, int4* __restrict__ blist) {
   const int lane = threadIdx.x & 31;
   for (int64_t i = global_warp(); i < n_rows; i += grid_warps()) {
     const int64_t I = rcl[i];
-    const int a = ratom[i];
+    const int geo_r = roff[i] | ((int)row_bs[i] << 13);
     for (int64_t b = row_p[i] + lane; b < row_p[i + 1]; b += 32) {
       const int j = col[b];
       const int64_t t = pos[I * n_cc + ccl[j]];
-      tblk[t * (kMaxRowAtoms * kMaxColAtoms) + a * kMaxColAtoms + catom[j]] = (int32_t)b;
+      const int64_t slot = (int64_t)atomicAdd(reinterpret_cast<unsigned long long*>(&cnt[t]), 1ull);
+      if (FILL) {
+        const int geo = geo_r | (coff[j] << 7) | ((int)col_bs[j] << 20) | (catom[j] << 27);
+        const uint64_t o = (uint64_t)off[b];
+        blist[lbase[t] + slot] = make_int4((int)b, geo, (int)(uint32_t)o, (int)(uint32_t)(o >> 32));
+      }
     }
   }
 }
@@ -851,9 +1014,8 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_TRY(m.up(rc.first, &d_rcf)); LAMB_TRY(m.up(rc.atoms, &d_rca));
   LAMB_TRY(m.up(cc.of, &d_ccl)); LAMB_TRY(m.up(cc.idx, &d_catom)); LAMB_TRY(m.up(cc.off, &d_coff));
   LAMB_TRY(m.up(cc.first, &d_ccf)); LAMB_TRY(m.up(cc.atoms, &d_cca));
-  // per-cluster tables of the epilogue: row / column descriptors and exponents
-  std::vector<int32_t> h_rc_row((size_t)rc.n * kM, -1), h_rc_ab((size_t)rc.n * kMaxRowAtoms, 0);
-  std::vector<int32_t> h_cc_col((size_t)cc.n * kN, -1);
+  // per-cluster tables of the epilogue: column descriptors, row and column exponents
+  std::vector<int32_t> h_cc_col((size_t)cc.n * kN, 0);
   std::vector<int64_t> h_rc_elem((size_t)rc.n * kM, -1), h_cc_elem((size_t)cc.n * kN, -1);
   {
     std::vector<int64_t> rb(A->n_rows + 1, 0), cb(B->n_cols + 1, 0);
@@ -862,24 +1024,20 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
     for (int I = 0; I < rc.n; ++I)
       for (int a = 0; a < rc.first[I + 1] - rc.first[I]; ++a) {
         const int atom = rc.atoms[rc.first[I] + a], b = A->h_row_bs[atom], o = rc.off[atom];
-        h_rc_ab[(size_t)I * kMaxRowAtoms + a] = (b << 16) | o;
-        for (int pe = 0; pe < b; ++pe) {
-          h_rc_row[(size_t)I * kM + o + pe] = (a << 8) | pe;
-          h_rc_elem[(size_t)I * kM + o + pe] = rb[atom] + pe;
-        }
+        for (int pe = 0; pe < b; ++pe) h_rc_elem[(size_t)I * kM + o + pe] = rb[atom] + pe;
       }
     for (int J = 0; J < cc.n; ++J)
       for (int b = 0; b < cc.first[J + 1] - cc.first[J]; ++b) {
         const int atom = cc.atoms[cc.first[J] + b], w = B->h_col_bs[atom], o = cc.off[atom];
         for (int q = 0; q < w; ++q) {
-          h_cc_col[(size_t)J * kN + o + q] = (b << 16) | (q << 8) | (q == w - 1 ? 1 : 0);
+          h_cc_col[(size_t)J * kN + o + q] = (b << 1) | (q == w - 1 ? 1 : 0);
           h_cc_elem[(size_t)J * kN + o + q] = cb[atom] + q;
         }
       }
   }
-  int32_t *d_rc_row, *d_rc_ab, *d_cc_col, *d_rc_exp, *d_cc_exp;
+  int32_t *d_cc_col, *d_rc_exp, *d_cc_exp;
   int64_t *d_rc_elem, *d_cc_elem;
-  LAMB_TRY(m.up(h_rc_row, &d_rc_row)); LAMB_TRY(m.up(h_rc_ab, &d_rc_ab)); LAMB_TRY(m.up(h_cc_col, &d_cc_col));
+  LAMB_TRY(m.up(h_cc_col, &d_cc_col));
   LAMB_TRY(m.up(h_rc_elem, &d_rc_elem)); LAMB_TRY(m.up(h_cc_elem, &d_cc_elem));
   LAMB_TRY(m.alloc(&d_rc_exp, (int64_t)rc.n * kM)); LAMB_TRY(m.alloc(&d_cc_exp, (int64_t)cc.n * kN));
   k_tc_cluster_exp<<<grid_for((int64_t)rc.n * kM), 256, 0, ctx->stream>>>((int64_t)rc.n * kM, d_rc_elem, mp.ea, d_rc_exp);
@@ -941,18 +1099,28 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_CUDA(ctx, cudaMemcpyAsync(&n_tiles, pos + n_map, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   int2* tiles;
-  int32_t *tblk, *krows;
-  int64_t *ecnt, *ebase;
+  int32_t* krows;
+  int64_t *ecnt, *ebase, *lcnt, *lbase;
+  int4* blist;
   LAMB_TRY(m.alloc(&tiles, n_tiles));
-  LAMB_TRY(m.alloc(&tblk, n_tiles * (kMaxRowAtoms * kMaxColAtoms)));
+  LAMB_TRY(m.alloc(&lcnt, n_tiles + 1));
+  LAMB_TRY(m.alloc(&lbase, n_tiles + 1));
+  LAMB_TRY(m.alloc(&blist, C->nnz));
   LAMB_TRY(m.alloc(&krows, n_tiles));
   LAMB_TRY(m.alloc(&ecnt, n_tiles + 1));
   LAMB_TRY(m.alloc(&ebase, n_tiles + 1));
   k_tc_tile_list<<<grid_for(n_map, 256), 256, 0, ctx->stream>>>(n_map, cc.n, flag, pos, tiles);
   LAMB_LAUNCHED(ctx);
-  LAMB_CUDA(ctx, cudaMemsetAsync(tblk, 0xff, sizeof(int32_t) * (size_t)n_tiles * kMaxRowAtoms * kMaxColAtoms, ctx->stream));
-  k_tc_tile_blocks<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, d_rcl, d_ratom,
-                                                                          d_ccl, d_catom, cc.n, pos, tblk);
+  LAMB_CUDA(ctx, cudaMemsetAsync(lcnt, 0, sizeof(int64_t) * (size_t)(n_tiles + 1), ctx->stream));
+  k_tc_tile_blocks<false><<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(
+      C->n_rows, C->row_p, C->col, C->off, C->row_bs, C->col_bs, d_rcl, d_roff, d_ccl, d_coff, d_catom, cc.n, pos, lcnt,
+      nullptr, nullptr);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, lcnt, lbase, n_tiles + 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(lcnt, 0, sizeof(int64_t) * (size_t)(n_tiles + 1), ctx->stream));
+  k_tc_tile_blocks<true><<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(
+      C->n_rows, C->row_p, C->col, C->off, C->row_bs, C->col_bs, d_rcl, d_roff, d_ccl, d_coff, d_catom, cc.n, pos, lcnt,
+      lbase, blist);
   LAMB_LAUNCHED(ctx);
   LAMB_CUDA(ctx, cudaMemsetAsync(ecnt + n_tiles, 0, sizeof(int64_t), ctx->stream));
   k_tc_tile_k<false><<<grid_for(32ll * n_tiles, 256), 256, 0, ctx->stream>>>(
@@ -989,8 +1157,8 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   g.pan_a = pan_a; g.plane_a = plane_a; g.pan_b = pan_b; g.plane_b = plane_b;
   g.rc_first = d_rcf; g.rc_atoms = d_rca; g.cc_first = d_ccf; g.cc_atoms = d_cca;
   g.row_bs = C->row_bs; g.col_bs = C->col_bs; g.rbase = mp.rbase; g.cbase = mp.cbase; g.ea = mp.ea; g.eb = mp.eb;
-  g.tblk = tblk; g.c_off = C->off; g.c_data = C->data; g.c_nrm = c_nrm; g.err = d_err;
-  g.rc_row = d_rc_row; g.rc_exp = d_rc_exp; g.rc_ab = d_rc_ab; g.cc_col = d_cc_col; g.cc_exp = d_cc_exp;
+  g.blist = blist; g.lbase = lbase; g.c_data = C->data; g.c_nrm = c_nrm; g.err = d_err;
+  g.rc_exp = d_rc_exp; g.cc_col = d_cc_col; g.cc_exp = d_cc_exp;
   LAMB_CUDA(ctx, cudaFuncSetAttribute(k_tc_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
