@@ -33,20 +33,21 @@
 // would skip are included (they are bounded by eps each); the C pattern is
 // the filtered one, so only C blocks of the pattern are written.
 //
-// Kernel roles (one CTA of 256 threads per SM, persistent over the tiles):
-//   warps 0-2  producers: gather the tile's K rows, 32 per pipeline stage
-//              (two warps the A chunks, one warp the B chunks);
-//   warp 3     loads each tile's inner-atom list one tile ahead, allocates
+// Kernel roles (one CTA of 352 threads per SM, persistent over the tiles):
+//   warps 0-5  producers: gather the tile's K rows, 32 per pipeline stage
+//              (four warps the A chunks, two warps the B chunks);
+//   warp 6     loads each tile's inner-atom list one tile ahead, allocates
 //              the tensor memory (6 levels x 64 columns in 512) and from one
-//              lane issues S(S+1)/2 MMAs (M=128, N=64, K=32) per stage;
-//   warps 4-7  epilogue: tensor memory -> registers (the six levels of a
-//              column recombined exactly in two int64 sums, then FP64),
-//              scaling into a staging tile in shared memory, per-row
-//              partial sums of squares per column atom; then every C block
-//              of the tile copied out in its storage order (contiguous
-//              stores, one warp a block) and its norm summed from the row
-//              partials.  The tile's block list (built before the kernel)
-//              and exponents are loaded one tile ahead into registers.
+//              lane issues nine MMAs (M=128, K=32, N=64..256) per stage,
+//              one per A digit plane and run of up to four B digit planes;
+//   warps 7-10 epilogue: tensor memory -> FP64 staging tile in shared
+//              memory (the six levels of a column recombined exactly in two
+//              int64 sums), then column scaling and per-row partial sums of
+//              squares per column atom; every C block of the tile copied out
+//              in its storage order (contiguous stores, one warp a block)
+//              and its norm summed from the row partials.  The tile's block
+//              list (built before the kernel) and exponents are loaded one
+//              tile ahead into registers.
 // Every wait on an mbarrier is bounded (2 s of %globaltimer); on a timeout
 // the kernel records an error code, every role stops, and the host returns
 // an error status.
@@ -82,8 +83,13 @@ constexpr double kBiasD = 6755399441055744.0;
 // Exponents up to this size scale by multiplying with exact powers of two
 // (no intermediate can under- or overflow); larger ones go through ldexp.
 constexpr int kExactExp = 500;
-constexpr int kTileThreads = 256;
-constexpr int kProducers = 96;
+constexpr int kProdWarps = 6;                 // warps 0-5: producers
+constexpr int kProducers = 32 * kProdWarps;
+constexpr int kMmaWarp = kProdWarps;          // warp 6: entry loader and MMA issuer
+constexpr int kEpiWarp0 = kMmaWarp + 1;       // warps 7-10: epilogue
+constexpr int kTileThreads = 32 * (kEpiWarp0 + 4);
+constexpr int kUnits = 32 * (8 + 4);          // 16-byte (row, chunk) copies of a stage and plane
+static_assert(kUnits % kProducers == 0, "units split evenly over the producers");
 constexpr int kTmemCols = 512;
 constexpr int64_t kRowMask = (1 << 25) - 1;  // panel row of an entry (bk in the top 7 bits)
 // Level accumulators stay exact while (K rows) * S * 127^2 < 2^31.
@@ -108,14 +114,16 @@ struct __align__(16) TileSmem {
   int32_t ent_b[2][kMaxEnt];
   uint16_t ent_pre[2][kMaxEnt + 8];  // first K row of every entry (K rows < 2^16)
   int32_t ent_n[2];
+  int32_t ent_k[2];  // K rows of the tile
   // epilogue tables of the current tile
-  long long blk_off[kMaxBlocks];  // data offset of each C block of the tile
-  int32_t blk_id[kMaxBlocks];     // its index in C
-  int32_t blk_geom[kMaxBlocks];   // its first tile row, first tile column, sizes, column atom
+  long long boff[kMaxBlocks];     // data offset of C block (row atom a, column atom b) at a * 16 + b, or -1
+  int32_t blk_id[kMaxBlocks];     // C blocks of the tile in list order: index in C
+  int32_t blk_geom[kMaxBlocks];   // and geometry (first tile row | bi << 7 | row atom << 14 | column atom << 19)
   double col_scale[kN];           // 2^exponent of every tile column (when not wide)
   int32_t col_exp[kN];
-  int32_t col_info[kN];           // column atom << 1 | last column of the atom (0 for padding)
+  int32_t col_atom[kMaxColAtoms]; // first tile column | width << 8 of every column atom
   int32_t n_blk;
+  int32_t n_col_atoms;
   unsigned long long bar_full[kStages], bar_empty[kStages];
   unsigned long long bar_tmem_full, bar_tmem_empty, bar_ent_full[2], bar_ent_empty[2], bar_done;
   uint32_t tmem_base;
@@ -151,12 +159,14 @@ struct TcArgs {
   // each (C block index, geometry, data offset low, high word)
   const int4* blist;
   const int64_t* lbase;
-  // per row cluster and tile row m the row's exponent (0 for padding)
+  // per row cluster and tile row m: the row's exponent (0 for padding) and
+  // (row atom << 16 | element << 8 | block size) or -1 for padding
   const int32_t* rc_exp;
-  // per column cluster and tile column n: the column's exponent, and
-  // (column atom << 1 | last column of the atom) or 0 for padding
+  const int32_t* rc_row;
+  // per column cluster and tile column n the column's exponent; per column
+  // atom (first tile column | width << 8)
   const int32_t* cc_exp;
-  const int32_t* cc_col;
+  const int32_t* cc_ab;
   double* c_data;
   double* c_nrm;
   int* err;
@@ -297,7 +307,10 @@ __device__ __forceinline__ uint32_t b_swz(int kk, int c) { return (uint32_t)(kk 
 // ---- the tile kernel ------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  // 1024-byte aligned base by pointer arithmetic on the shared array, so that
+  // the compiler keeps the shared state space (shared loads and stores, not
+  // generic ones)
+  unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   unsigned char* stages = base;
   TileSmem* sm = reinterpret_cast<TileSmem*>(base + (size_t)kStages * kStageBytes);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -317,7 +330,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     sm->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 3) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm->tmem_base)),
                  "r"(kTmemCols)
                  : "memory");
@@ -329,11 +342,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
   const uint32_t tmem = sm->tmem_base;
   const int64_t n_tiles = g.n_tiles;
 
-  if (warp < 3) {
+  if (warp < kProdWarps) {
     // ================= producers =================
-    const int pt = tid;  // 0..95
+    const int pt = tid;  // 0..kProducers-1
     // A stage is 32 inner rows x (8 A chunks + 4 B chunks) of 16 bytes per
-    // digit plane: 384 (row, chunk) units, four per producer thread.  Units
+    // digit plane: 384 (row, chunk) units, two per producer thread.  Units
     // 0..255 are A (row u / 8, chunk u % 8), 256..383 are B (row v / 4,
     // chunk v % 4): consecutive lanes copy consecutive chunks of one panel
     // row, so a warp reads whole 128-byte (A) or 64-byte (B) rows.
@@ -343,31 +356,53 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       const int buf = (int)(local & 1);
       if (!bar_wait(&sm->bar_ent_full[buf], (uint32_t)((local >> 1) & 1), sm, g.err, kErrTimeoutEnt)) break;
       const int n = sm->ent_n[buf];
-      const int K = g.krows[t];
+      const int K = sm->ent_k[buf];
       const int nst = K > 0 ? (K + kK - 1) / kK : 1;
       const uint16_t* pre = sm->ent_pre[buf];
+      // last entry e with pre[e] <= kk (a binary search; only for stages
+      // where more than 31 entries start)
+      auto find = [&](int kk) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (pre[mid] <= kk) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+      };
+      int e0 = 0;  // the entry holding the stage's first inner row
       for (int s = 0; s < nst; ++s, ++gs) {
         const int stg = (int)(gs % kStages);
         if (!bar_wait(&sm->bar_empty[stg], (uint32_t)(((gs / kStages) & 1) ^ 1), sm, g.err, kErrTimeoutEmpty)) break;
         const uint32_t sa = smem_u32(stages + (size_t)stg * kStageBytes);
         const uint32_t sb = sa + kStageA;
         // lane r of every producer warp finds the panel rows of the stage's
-        // inner row r (one search per lane); the units take them by shuffle
+        // inner row r; the units take them by shuffle.  Lane j reads the
+        // start of entry e0 + j: the entries starting inside the stage set
+        // one bit each (starts are distinct, every entry has rows), and the
+        // entry of row r is e0 plus the starts at or before it.
         int my_a = 0, my_b = 0;
         {
-          const int kk = s * kK + lane;
+          const int r0 = s * kK, kk = r0 + lane;
+          const int j = e0 + lane;
+          const int P = j <= n ? (int)pre[j] : 0x10000;
+          const uint32_t mask = __reduce_or_sync(0xffffffffu, lane >= 1 && P < r0 + kK ? 1u << (P - r0) : 0u);
+          const bool at_end = __any_sync(0xffffffffu, lane >= 1 && P == r0 + kK);
+          const bool crowded = __shfl_sync(0xffffffffu, P, 31) < r0 + kK;  // starts beyond the 32 read
+          int e;
+          if (!crowded) {
+            e = e0 + __popc(mask & (0xffffffffu >> (31 - lane)));
+            e0 += __popc(mask) + (at_end ? 1 : 0);
+          } else {
+            e = find(kk < K ? kk : K - 1);
+            e0 = find(r0 + kK < K ? r0 + kK : K - 1);
+          }
           if (kk < K) {
-            int lo = 0, hi = n - 1;  // last entry e with pre[e] <= kk
-            while (lo < hi) {
-              const int mid = (lo + hi + 1) >> 1;
-              if (pre[mid] <= kk) lo = mid; else hi = mid - 1;
-            }
-            my_a = sm->ent_a[buf][lo] + (kk - pre[lo]);
-            my_b = sm->ent_b[buf][lo] + (kk - pre[lo]);
+            my_a = sm->ent_a[buf][e] + (kk - pre[e]);
+            my_b = sm->ent_b[buf][e] + (kk - pre[e]);
           }
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < kUnits / kProducers; ++i) {
           const int u = pt + kProducers * i;
           const bool is_a = u < 256;  // uniform over the warp
           const int row = is_a ? (u >> 3) : ((u - 256) >> 2);
@@ -390,17 +425,18 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       // the entry buffer of this tile may be refilled once every producer is past it
       bar_arrive(&sm->bar_ent_empty[buf]);
     }
-  } else if (warp >= 4) {
+  } else if (warp >= kEpiWarp0) {
     // ================= epilogue =================
-    const int et = tid - 128;       // 0..127: tile row m
-    const int ew = warp - 4;        // tensor-memory lane quarter
+    const int ew = warp & 3;        // tensor-memory lane quarter (warp id mod 4)
+    const int et = 32 * ew + lane;  // tile row m
     // Tables of the next tile, loaded into registers while the current tile
-    // is copied out: its row exponent (this thread's row), column exponent
-    // and column info (threads < kN), block count and up to kMaxBlocks / 128
-    // block-list entries per thread.  The list bounds of the tile after next
-    // are loaded one tile earlier still, so no load waits on another.
+    // is written out: this thread's row exponent and row descriptor, the
+    // column exponents (threads < kN), column atoms (threads < 16) and
+    // count, block count and up to kMaxBlocks / 128 block-list entries per
+    // thread.  The list bounds and clusters of the tile after next are
+    // loaded one tile earlier still, so no load waits on another.
     constexpr int kBlkRegs = kMaxBlocks / 128;
-    int nx_er = 0, nx_ec = 0, nx_ci = 0, nx_nb = 0;
+    int nx_er = 0, nx_ri = -1, nx_ec = 0, nx_cab = 0, nx_nca = 0, nx_nb = 0;
     int4 nx_b[kBlkRegs];
     int64_t lb_lo = 0, lb_hi = 0;  // list bounds of the tile being prefetched
     int2 lb_tile = make_int2(0, 0);  // and its clusters
@@ -412,10 +448,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     auto prefetch = [&]() {
       const int I = lb_tile.x, J = lb_tile.y;
       nx_er = g.rc_exp[(int64_t)I * kM + et];
-      if (et < kN) {
-        nx_ec = g.cc_exp[(int64_t)J * kN + et];
-        nx_ci = g.cc_col[(int64_t)J * kN + et];
-      }
+      nx_ri = g.rc_row[(int64_t)I * kM + et];
+      if (et < kN) nx_ec = g.cc_exp[(int64_t)J * kN + et];
+      if (et < kMaxColAtoms) nx_cab = g.cc_ab[(int64_t)J * kMaxColAtoms + et];
+      nx_nca = g.cc_first[J + 1] - g.cc_first[J];
       nx_nb = (int)(lb_hi - lb_lo);
 #pragma unroll
       for (int j = 0; j < kBlkRegs; ++j) {
@@ -426,32 +462,41 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     // Writes the prefetched tables to shared memory; returns whether some
     // exponent of the tile lies beyond kExactExp (the same for every thread).
     auto publish = [&]() -> bool {
+#pragma unroll
+      for (int j = 0; j < kBlkRegs; ++j) sm->boff[et + 128 * j] = -1;
       if (et < kN) {
         sm->col_exp[et] = nx_ec;
         sm->col_scale[et] = pow2(nx_ec < -kExactExp || nx_ec > kExactExp ? 0 : nx_ec);
-        sm->col_info[et] = nx_ci;
       }
+      if (et < kMaxColAtoms) sm->col_atom[et] = nx_cab;
+      if (et == 0) {
+        sm->n_blk = nx_nb;
+        sm->n_col_atoms = nx_nca;
+      }
+      named_sync(2, 128);  // every slot reset before the blocks are entered
 #pragma unroll
       for (int j = 0; j < kBlkRegs; ++j) {
         const int k = et + 128 * j;
         if (k < nx_nb) {
+          const int geo = nx_b[j].y;
           sm->blk_id[k] = nx_b[j].x;
-          sm->blk_geom[k] = nx_b[j].y;
-          sm->blk_off[k] = (long long)(((uint64_t)(uint32_t)nx_b[j].w << 32) | (uint32_t)nx_b[j].z);
+          sm->blk_geom[k] = geo;
+          sm->boff[((geo >> 14) & 31) * kMaxColAtoms + ((geo >> 19) & 15)] =
+              (long long)(((uint64_t)(uint32_t)nx_b[j].w << 32) | (uint32_t)nx_b[j].z);
         }
       }
-      if (et == 0) sm->n_blk = nx_nb;
       const bool w = nx_er < -kExactExp || nx_er > kExactExp || (et < kN && (nx_ec < -kExactExp || nx_ec > kExactExp));
       return named_sync_or(2, 128, w);
     };
     int64_t local = 0;
     bool wide = false;
-    int er = 0;
+    int er = 0, ri = -1;  // this thread's row: exponent and descriptor
     if ((int64_t)blockIdx.x < n_tiles) {
       bounds(blockIdx.x);
       prefetch();
       bounds(blockIdx.x + (int64_t)gridDim.x);
       er = nx_er;
+      ri = nx_ri;
       wide = publish();
     }
     for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
@@ -494,70 +539,48 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
         prefetch();
         bounds(t + 2 * (int64_t)gridDim.x);
       }
-      // ---- column scaling in place and the row partials of the sums of
-      // squares (column order within each column atom) ----
-      {
+      // ---- write-out: each thread writes its tile row into the C blocks of
+      // its row atom, one column atom after the other (a block's column is
+      // bi consecutive doubles, so a warp's store covers its rows' runs),
+      // scaling by the column's power of two, and keeps the row's sum of
+      // squares per column atom for the block norms ----
+      if (ri >= 0) {
+        const int a = ri >> 16, pe = (ri >> 8) & 0xff, bi = ri & 0xff;
+        const int nca = sm->n_col_atoms;
         double* part = sm->part + et * kPartStride;
-        double run = 0.0;
-        if (!wide) {
-#pragma unroll 1
-          for (int n = 0; n < kN; n += 4) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const double y = row[(n + c) ^ sw] * sm->col_scale[n + c];
-              row[(n + c) ^ sw] = y;
-              run = __fma_rn(y, y, run);
-              const int ci = sm->col_info[n + c];
-              if (ci & 1) {
-                part[ci >> 1] = run;
-                run = 0.0;
+        for (int b = 0; b < nca; ++b) {
+          const int cab = sm->col_atom[b];
+          const int c0 = cab & 0xff, bj = cab >> 8;
+          const long long bo = sm->boff[a * kMaxColAtoms + b];
+          double sq = 0.0;
+          if (bo >= 0) {
+            double* __restrict__ dst = g.c_data + bo + pe;
+            if (!wide) {
+#pragma unroll 4
+              for (int q = 0; q < bj; ++q) {
+                const int n = c0 + q;
+                const double v = row[n ^ sw] * sm->col_scale[n];
+                dst[q * bi] = v;
+                sq = __fma_rn(v, v, sq);
+              }
+            } else {  // rare: exponents beyond kExactExp, scaled out of line
+              for (int q = 0; q < bj; ++q) {
+                const int n = c0 + q;
+                const double v = scale_wide(row[n ^ sw], er + sm->col_exp[n]);
+                dst[q * bi] = v;
+                sq = __fma_rn(v, v, sq);
               }
             }
           }
-        } else {  // rare: exponents beyond kExactExp, scaled out of line
-          for (int n = 0; n < kN; ++n) {
-            const double y = scale_wide(row[n ^ sw], er + sm->col_exp[n]);
-            row[n ^ sw] = y;
-            run = __fma_rn(y, y, run);
-            const int ci = sm->col_info[n];
-            if (ci & 1) {
-              part[ci >> 1] = run;
-              run = 0.0;
-            }
-          }
+          part[b] = sq;
         }
       }
       named_sync(2, 128);
-      // ---- copy-out: one warp per C block, elements in storage order
-      // (column-major: element e is (e % bi, e / bi)), contiguous stores ----
-      const int nb = sm->n_blk;
-      for (int k = ew; k < nb; k += 4) {
-        const int geo = sm->blk_geom[k];
-        const int r0 = geo & 127, c0 = (geo >> 7) & 63, bi = (geo >> 13) & 127, bj = (geo >> 20) & 127;
-        double* __restrict__ out = g.c_data + sm->blk_off[k];
-        // lane / bi and 32 / bi: the float quotient is at least 0.5 / bi away
-        // from the next integer, far more than its rounding error
-        const float rcp = __frcp_rn((float)bi);
-        int q = (int)(((float)lane + 0.5f) * rcp);
-        int pe = lane - q * bi;
-        const int step_q = (int)(32.5f * rcp), step_r = 32 - step_q * bi;
-        const int ne = bi * bj;
-#pragma unroll 4
-        for (int e = lane; e < ne; e += 32) {
-          const int mm = r0 + pe, nn = c0 + q;
-          out[e] = sm->stg[mm * kN + (nn ^ (mm & 15))];
-          pe += step_r;
-          q += step_q;
-          if (pe >= bi) {
-            pe -= bi;
-            ++q;
-          }
-        }
-      }
       // ---- block norms: rows of the block in ascending order ----
+      const int nb = sm->n_blk;
       for (int k = et; k < nb; k += 128) {
         const int geo = sm->blk_geom[k];
-        const int r0 = geo & 127, bi = (geo >> 13) & 127, cb = (geo >> 27) & 15;
+        const int r0 = geo & 127, bi = (geo >> 7) & 127, cb = (geo >> 19) & 15;
         double sq = 0.0;
         for (int pe = 0; pe < bi; ++pe) sq += sm->part[(r0 + pe) * kPartStride + cb];
         g.c_nrm[sm->blk_id[k]] = __dsqrt_rn(sq);
@@ -565,11 +588,12 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       named_sync(2, 128);  // the staging tile and the tables are free again
       if (has_next) {
         er = nx_er;
+        ri = nx_ri;
         wide = publish();
       }
     }
   } else {
-    // ================= warp 3: entry loader (all lanes) and MMA issuer (lane 0) =================
+    // ================= entry loader (all lanes) and MMA issuer (lane 0) =================
     // Entries of tile `local` go to buffer local % 2.  The next tile's
     // entries are loaded into registers when a tile starts and written to
     // shared memory once the tile's tensor memory is free (the loads fly
@@ -579,14 +603,23 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     bool ok = true;
     constexpr int kEntRegs = kMaxEnt / 32;
     uint2 pre_x[kEntRegs];
-    int pre_n = 0;
-    auto prefetch = [&](int64_t t) {
-      pre_n = (int)g.ent_cnt[t];
-      const int64_t eb = g.ent_base[t];
+    int pre_n = 0, pre_k = 0, cur_k = 0;
+    // entry count, base and K rows of the tile to prefetch next, loaded one
+    // tile earlier so that the entry loads wait on nothing
+    int64_t nb_cnt = 0, nb_base = 0;
+    int nb_k = 0;
+    auto bounds = [&](int64_t t) {
+      nb_cnt = t < n_tiles ? g.ent_cnt[t] : 0;
+      nb_base = t < n_tiles ? g.ent_base[t] : 0;
+      nb_k = t < n_tiles ? g.krows[t] : 0;
+    };
+    auto prefetch = [&]() {
+      pre_n = (int)nb_cnt;
+      pre_k = nb_k;
 #pragma unroll
       for (int j = 0; j < kEntRegs; ++j) {
         const int e = lane + 32 * j;
-        pre_x[j] = e < pre_n ? g.ent[eb + e] : make_uint2(0u, 0u);
+        pre_x[j] = e < pre_n ? g.ent[nb_base + e] : make_uint2(0u, 0u);
       }
     };
     auto publish = [&](int64_t lidx) -> bool {
@@ -616,20 +649,27 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       if (lane == 0) {
         sm->ent_pre[buf][pre_n] = (uint16_t)carry;
         sm->ent_n[buf] = pre_n;
+        sm->ent_k[buf] = pre_k;
       }
       __syncwarp();
       bar_arrive(&sm->bar_ent_full[buf]);
       return true;
     };
     if ((int64_t)blockIdx.x < n_tiles) {
-      prefetch(blockIdx.x);
+      bounds(blockIdx.x);
+      prefetch();
+      bounds(blockIdx.x + (int64_t)gridDim.x);
       ok = publish(0);
     }
     for (int64_t t = blockIdx.x; ok && t < n_tiles && !sm->abort; t += gridDim.x, ++local_mma) {
       const bool has_next = t + gridDim.x < n_tiles;
-      if (has_next) prefetch(t + gridDim.x);
+      cur_k = pre_k;  // K rows of tile t (published with its entries)
+      if (has_next) {
+        prefetch();
+        bounds(t + 2 * (int64_t)gridDim.x);
+      }
       bool published = !has_next;
-      const int K = g.krows[t];
+      const int K = cur_k;
       const int nst = K > 0 ? (K + kK - 1) / kK : 1;
       // tensor memory is free once the epilogue has read the previous tile
       if (!bar_wait(&sm->bar_tmem_empty, (uint32_t)((local_mma & 1) ^ 1), sm, g.err, kErrTimeoutTmemEmpty)) break;
@@ -679,7 +719,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 3)
+  if (warp == kMmaWarp)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
@@ -831,26 +871,26 @@ __global__ void k_tc_tile_list(int64_t n_map, int32_t n_cc, const int64_t* __res
 // C blocks of every tile.  Count pass: blocks per tile.  Fill pass: one
 // list entry per block at lbase[t] + (arrival order within the tile), each
 // (block index, geometry, data offset) with geometry = first tile row |
-// first tile column << 7 | bi << 13 | bj << 20 | column atom << 27.  The
-// order within a tile only decides which warp copies which block.
+// bi << 7 | row atom << 14 | column atom << 19.  The order within a tile
+// decides nothing but which thread computes which norm.
 template <bool FILL>
 __global__ void k_tc_tile_blocks(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                                  const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
-                                 const int8_t* __restrict__ col_bs, const int32_t* __restrict__ rcl,
-                                 const int32_t* __restrict__ roff, const int32_t* __restrict__ ccl,
-                                 const int32_t* __restrict__ coff, const int32_t* __restrict__ catom, int32_t n_cc,
+                                 const int32_t* __restrict__ rcl, const int32_t* __restrict__ roff,
+                                 const int32_t* __restrict__ ratom, const int32_t* __restrict__ ccl,
+                                 const int32_t* __restrict__ catom, int32_t n_cc,
                                  const int64_t* __restrict__ pos, int64_t* __restrict__ cnt,
                                  const int64_t* __restrict__ lbase, int4* __restrict__ blist) {
   const int lane = threadIdx.x & 31;
   for (int64_t i = global_warp(); i < n_rows; i += grid_warps()) {
     const int64_t I = rcl[i];
-    const int geo_r = roff[i] | ((int)row_bs[i] << 13);
+    const int geo_r = roff[i] | ((int)row_bs[i] << 7) | (ratom[i] << 14);
     for (int64_t b = row_p[i] + lane; b < row_p[i + 1]; b += 32) {
       const int j = col[b];
       const int64_t t = pos[I * n_cc + ccl[j]];
       const int64_t slot = (int64_t)atomicAdd(reinterpret_cast<unsigned long long*>(&cnt[t]), 1ull);
       if (FILL) {
-        const int geo = geo_r | (coff[j] << 7) | ((int)col_bs[j] << 20) | (catom[j] << 27);
+        const int geo = geo_r | (catom[j] << 19);
         const uint64_t o = (uint64_t)off[b];
         blist[lbase[t] + slot] = make_int4((int)b, geo, (int)(uint32_t)o, (int)(uint32_t)(o >> 32));
       }
@@ -1014,8 +1054,8 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_TRY(m.up(rc.first, &d_rcf)); LAMB_TRY(m.up(rc.atoms, &d_rca));
   LAMB_TRY(m.up(cc.of, &d_ccl)); LAMB_TRY(m.up(cc.idx, &d_catom)); LAMB_TRY(m.up(cc.off, &d_coff));
   LAMB_TRY(m.up(cc.first, &d_ccf)); LAMB_TRY(m.up(cc.atoms, &d_cca));
-  // per-cluster tables of the epilogue: column descriptors, row and column exponents
-  std::vector<int32_t> h_cc_col((size_t)cc.n * kN, 0);
+  // per-cluster tables of the epilogue: row and column-atom descriptors, row and column exponents
+  std::vector<int32_t> h_rc_row((size_t)rc.n * kM, -1), h_cc_ab((size_t)cc.n * kMaxColAtoms, 0);
   std::vector<int64_t> h_rc_elem((size_t)rc.n * kM, -1), h_cc_elem((size_t)cc.n * kN, -1);
   {
     std::vector<int64_t> rb(A->n_rows + 1, 0), cb(B->n_cols + 1, 0);
@@ -1024,20 +1064,22 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
     for (int I = 0; I < rc.n; ++I)
       for (int a = 0; a < rc.first[I + 1] - rc.first[I]; ++a) {
         const int atom = rc.atoms[rc.first[I] + a], b = A->h_row_bs[atom], o = rc.off[atom];
-        for (int pe = 0; pe < b; ++pe) h_rc_elem[(size_t)I * kM + o + pe] = rb[atom] + pe;
+        for (int pe = 0; pe < b; ++pe) {
+          h_rc_row[(size_t)I * kM + o + pe] = (a << 16) | (pe << 8) | b;
+          h_rc_elem[(size_t)I * kM + o + pe] = rb[atom] + pe;
+        }
       }
     for (int J = 0; J < cc.n; ++J)
       for (int b = 0; b < cc.first[J + 1] - cc.first[J]; ++b) {
         const int atom = cc.atoms[cc.first[J] + b], w = B->h_col_bs[atom], o = cc.off[atom];
-        for (int q = 0; q < w; ++q) {
-          h_cc_col[(size_t)J * kN + o + q] = (b << 1) | (q == w - 1 ? 1 : 0);
-          h_cc_elem[(size_t)J * kN + o + q] = cb[atom] + q;
-        }
+        h_cc_ab[(size_t)J * kMaxColAtoms + b] = o | (w << 8);
+        for (int q = 0; q < w; ++q) h_cc_elem[(size_t)J * kN + o + q] = cb[atom] + q;
       }
   }
-  int32_t *d_cc_col, *d_rc_exp, *d_cc_exp;
+  int32_t *d_rc_row, *d_cc_ab, *d_rc_exp, *d_cc_exp;
   int64_t *d_rc_elem, *d_cc_elem;
-  LAMB_TRY(m.up(h_cc_col, &d_cc_col));
+  LAMB_TRY(m.up(h_rc_row, &d_rc_row));
+  LAMB_TRY(m.up(h_cc_ab, &d_cc_ab));
   LAMB_TRY(m.up(h_rc_elem, &d_rc_elem)); LAMB_TRY(m.up(h_cc_elem, &d_cc_elem));
   LAMB_TRY(m.alloc(&d_rc_exp, (int64_t)rc.n * kM)); LAMB_TRY(m.alloc(&d_cc_exp, (int64_t)cc.n * kN));
   k_tc_cluster_exp<<<grid_for((int64_t)rc.n * kM), 256, 0, ctx->stream>>>((int64_t)rc.n * kM, d_rc_elem, mp.ea, d_rc_exp);
@@ -1113,14 +1155,14 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_LAUNCHED(ctx);
   LAMB_CUDA(ctx, cudaMemsetAsync(lcnt, 0, sizeof(int64_t) * (size_t)(n_tiles + 1), ctx->stream));
   k_tc_tile_blocks<false><<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(
-      C->n_rows, C->row_p, C->col, C->off, C->row_bs, C->col_bs, d_rcl, d_roff, d_ccl, d_coff, d_catom, cc.n, pos, lcnt,
-      nullptr, nullptr);
+      C->n_rows, C->row_p, C->col, C->off, C->row_bs, d_rcl, d_roff, d_ratom, d_ccl, d_catom, cc.n, pos, lcnt, nullptr,
+      nullptr);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, lcnt, lbase, n_tiles + 1));
   LAMB_CUDA(ctx, cudaMemsetAsync(lcnt, 0, sizeof(int64_t) * (size_t)(n_tiles + 1), ctx->stream));
   k_tc_tile_blocks<true><<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(
-      C->n_rows, C->row_p, C->col, C->off, C->row_bs, C->col_bs, d_rcl, d_roff, d_ccl, d_coff, d_catom, cc.n, pos, lcnt,
-      lbase, blist);
+      C->n_rows, C->row_p, C->col, C->off, C->row_bs, d_rcl, d_roff, d_ratom, d_ccl, d_catom, cc.n, pos, lcnt, lbase,
+      blist);
   LAMB_LAUNCHED(ctx);
   LAMB_CUDA(ctx, cudaMemsetAsync(ecnt + n_tiles, 0, sizeof(int64_t), ctx->stream));
   k_tc_tile_k<false><<<grid_for(32ll * n_tiles, 256), 256, 0, ctx->stream>>>(
@@ -1158,7 +1200,7 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   g.rc_first = d_rcf; g.rc_atoms = d_rca; g.cc_first = d_ccf; g.cc_atoms = d_cca;
   g.row_bs = C->row_bs; g.col_bs = C->col_bs; g.rbase = mp.rbase; g.cbase = mp.cbase; g.ea = mp.ea; g.eb = mp.eb;
   g.blist = blist; g.lbase = lbase; g.c_data = C->data; g.c_nrm = c_nrm; g.err = d_err;
-  g.rc_exp = d_rc_exp; g.cc_col = d_cc_col; g.cc_exp = d_cc_exp;
+  g.rc_exp = d_rc_exp; g.rc_row = d_rc_row; g.cc_exp = d_cc_exp; g.cc_ab = d_cc_ab;
   LAMB_CUDA(ctx, cudaFuncSetAttribute(k_tc_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -1188,7 +1230,10 @@ namespace tc {
 template <int N>
 __global__ void __launch_bounds__(128, 1) k_tc_probe(int iters, int* err) {
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  // 1024-byte aligned base by pointer arithmetic on the shared array, so that
+  // the compiler keeps the shared state space (shared loads and stores, not
+  // generic ones)
+  unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   __shared__ unsigned long long bar;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
