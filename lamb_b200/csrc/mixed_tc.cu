@@ -291,10 +291,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
         "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int (&v)[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-               : "r"(taddr));
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -501,7 +503,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
     }
     for (int64_t t = blockIdx.x; t < n_tiles && !sm->abort; t += gridDim.x, ++local) {
       const bool has_next = t + gridDim.x < n_tiles;
-      // ---- accumulators: tensor memory -> staging tile, 8 columns a round
+      // ---- accumulators: tensor memory -> staging tile, 16 columns a round
       // (a rolled loop: the epilogue's code stays small next to the other
       // roles' in the instruction cache).  Per column the six level sums v_L
       // recombine as (v0 254^2 + v1 254 + v2) w_2 + (v3 254^2 + v4 254 + v5) w_5
@@ -519,13 +521,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
         const double w2 = kLevelW[2] * rs, w5 = kLevelW[5] * rs;
         const uint32_t lane_base = tmem + ((uint32_t)(32 * ew) << 16);
 #pragma unroll 1
-        for (int c0 = 0; c0 < kN; c0 += 8) {
-          int v[kS][8];
+        for (int c0 = 0; c0 < kN; c0 += 16) {
+          int v[kS][16];
 #pragma unroll
-          for (int L = 0; L < kS; ++L) tmem_ld8(lane_base + (uint32_t)(64 * L + c0), v[L]);
+          for (int L = 0; L < kS; ++L) tmem_ld16(lane_base + (uint32_t)(64 * L + c0), v[L]);
           tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 8; ++c) {
+          for (int c = 0; c < 16; ++c) {
             const long long hi = kBias + (long long)v[0][c] * 64516 + (long long)v[1][c] * 254 + v[2][c];
             const long long lo = kBias + (long long)v[3][c] * 64516 + (long long)v[4][c] * 254 + v[5][c];
             const double hd = __longlong_as_double(hi) - kBiasD, ld = __longlong_as_double(lo) - kBiasD;
@@ -674,10 +676,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
       // tensor memory is free once the epilogue has read the previous tile
       if (!bar_wait(&sm->bar_tmem_empty, (uint32_t)((local_mma & 1) ^ 1), sm, g.err, kErrTimeoutTmemEmpty)) break;
       tc_fence_after();
-      if (!published) {  // the prefetch has landed meanwhile
-        published = true;
-        if (!(ok = publish(local_mma + 1))) break;
-      }
       for (int s = 0; s < nst; ++s, ++gs) {
         const int stg = (int)(gs % kStages);
         if (!bar_wait(&sm->bar_full[stg], (uint32_t)((gs / kStages) & 1), sm, g.err, kErrTimeoutFull)) { ok = false; break; }
@@ -706,6 +704,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tc_tiles(TcArgs g) {
           mma_commit(&sm->bar_empty[stg]);
         }
         __syncwarp();
+        if (!published) {  // after the tile's first MMAs: the next tile's entries (loaded meanwhile)
+          published = true;
+          if (!(ok = publish(local_mma + 1))) break;
+        }
       }
       if (!ok) break;
       if (lane == 0) mma_commit(&sm->bar_tmem_full);
