@@ -286,14 +286,16 @@ def run_mixed_leg(ctx, lib, local, da, db, dc, wl, args, flops, ms_fp64):
         f = lib.lamb_probe_int8_tcgen05_tops
         f.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
         peak = ctypes.c_double()
-        ctx.check(f(local, 64, 5, ctypes.byref(peak)))
+        ctx.check(f(local, 0, 5, ctypes.byref(peak)))
         achieved = t_ops / (ms_num * 1e-3) / 1e12
-        out["path"] = ("tcgen05.mma kind::i8 (M=128, N=64, K=32) on 128x64 spatial cluster tiles, six base-254 "
-                       "digits per operand, 21 digit-pair products into six int32 TMEM level accumulators, FP64 "
-                       "recombination")
+        out["path"] = ("tcgen05.mma kind::i8 (M=128, K=32, N=64..256: one MMA per A digit plane and run of up to "
+                       "four B digit planes, nine per 32-row stage) on 128x64 spatial cluster tiles, six base-254 "
+                       "digits per operand, 21 digit-pair products into six int32 TMEM level accumulators, exact "
+                       "int64 level recombination, FP64 scaling")
         out["roofline"] = {"bound": "tensor", "kernel": "k_tc_tiles", "achieved": achieved, "peak": peak.value,
                            "unit": "TOP/s (int8)", "frac": achieved / peak.value,
-                           "peak_source": "tcgen05 kind::i8 N=64 throughput probe on this GPU in this run",
+                           "peak_source": "tcgen05 kind::i8 probe issuing the tile kernel's own nine-MMA stage "
+                                          "(lamb_probe_int8_tcgen05_tops n=0) on this GPU in this run",
                            "tensor_ops_per_multiply": t_ops,
                            "useful_fraction": flops * s_m * (s_m + 1) / 2 / t_ops,
                            "note": "executed ops include the zero padding of the cluster tiles; useful_fraction = "

@@ -24,9 +24,10 @@ LAMB_API int32_t lamb_probe_int8_tops(int32_t device, int32_t reps, double* tops
 LAMB_API int32_t lamb_probe_bf16_tflops(int32_t device, int32_t reps, double* tflops);
 /* int8 throughput of the 5th-generation tensor cores as the mixed multiply's
  * tile kernel drives them: one CTA per SM issues tcgen05.mma kind::i8
- * (M = 128, K = 32, N = n: 64, the kernel's shape, or 256, the widest)
- * from shared memory into tensor-memory accumulators; best of `reps`
- * launches, TOP/s (1 op = 1 multiply or 1 add).  Allocates 4 bytes. */
+ * (M = 128, K = 32, N = n: 64 or 256, the widest; n = 0 issues the tile
+ * kernel's own stage, nine MMAs of N = 64 to 256 covering the 21 digit
+ * pairs) from shared memory into tensor-memory accumulators; best of
+ * `reps` launches, TOP/s (1 op = 1 multiply or 1 add).  Allocates 4 bytes. */
 LAMB_API int32_t lamb_probe_int8_tcgen05_tops(int32_t device, int32_t n, int32_t reps, double* tops);
 #ifdef __cplusplus
 }

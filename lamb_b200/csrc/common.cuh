@@ -238,6 +238,30 @@ __device__ __forceinline__ int row_subset(const int32_t* __restrict__ rsub_base,
   return m;
 }
 // Warp-per-row loops: global warp index and warp count of the grid.
+// Step of an element walk: e -> e + 32 moves (minor, major) of a block whose
+// minor extent is d by (32 % d, 32 / d) with a carry; the start (lane % d,
+// lane / d) and the steps come from one float quotient, exact for the
+// block sizes 1 <= d <= 127 because (lane + 0.5) / d lies at least 0.5 / d
+// from an integer.
+struct Walk {
+  int minor, major, step_minor, step_major, d;
+  __device__ __forceinline__ Walk(int d_, int lane) : d(d_) {
+    const float rcp = __frcp_rn((float)d_);
+    major = (int)(((float)lane + 0.5f) * rcp);
+    minor = lane - major * d_;
+    step_major = (int)(32.5f * rcp);
+    step_minor = 32 - step_major * d_;
+  }
+  __device__ __forceinline__ void next() {
+    minor += step_minor;
+    major += step_major;
+    if (minor >= d) {
+      minor -= d;
+      ++major;
+    }
+  }
+};
+
 __device__ __forceinline__ int64_t global_warp() { return ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ int64_t grid_warps() { return ((int64_t)gridDim.x * blockDim.x) >> 5; }
 

@@ -48,9 +48,12 @@ constexpr int64_t kLevelInnerMax7 = (int64_t)INT_MAX / (7 * 64 * 64);
 __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
 // ---- scales ----------------------------------------------------------------------------
-// Row exponents of A: one warp per block row; lanes take whole blocks and
-// merge their per-row maxima with shared-memory atomics (non-negative doubles
-// order like their bit patterns).
+// Row exponents of A: one warp per block row.  For bi <= 32 lane l keeps
+// the running max of element row l % bi over the columns l / bi, l / bi +
+// 32 / bi, ... of every block of the row (lanes of one column group read
+// consecutive elements); the lanes of one element row then merge through a
+// shared-memory atomic max (non-negative doubles order like their bit
+// patterns).  Larger blocks merge every element.
 __global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                           const int8_t* __restrict__ col_bs, const double* __restrict__ d,
@@ -62,13 +65,23 @@ __global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, con
     const int bi = row_bs[r];
     for (int p = lane; p < bi; p += 32) pm[wl][p] = 0ull;
     __syncwarp();
-    for (int64_t b = row_p[r] + lane; b < row_p[r + 1]; b += 32) {
-      const int bk = col_bs[col[b]];
-      const double* x = d + off[b];
-      for (int p = 0; p < bi; ++p) {
-        double m = 0.0;
-        for (int q = 0; q < bk; ++q) m = fmax(m, fabs(x[(int64_t)q * bi + p]));
-        atomicMax(&pm[wl][p], (unsigned long long)__double_as_longlong(m));
+    if (bi <= 32) {
+      const int G = 32 / bi, pe = lane % bi, g = lane / bi;
+      double m = 0.0;
+      if (g < G)
+        for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+          const int bk = col_bs[col[b]];
+          const double* x = d + off[b];
+          for (int kc = g; kc < bk; kc += G) m = fmax(m, fabs(x[pe + kc * bi]));
+        }
+      if (g < G) atomicMax(&pm[wl][pe], (unsigned long long)__double_as_longlong(m));
+    } else {
+      for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+        const int ne = bi * col_bs[col[b]];
+        const double* x = d + off[b];
+        Walk w(bi, lane);
+        for (int e = lane; e < ne; e += 32, w.next())
+          atomicMax(&pm[wl][w.minor], (unsigned long long)__double_as_longlong(fabs(x[e])));
       }
     }
     __syncwarp();
@@ -81,26 +94,43 @@ __global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, con
   }
 }
 
-// Column exponents of B: one warp per block row, lanes over its blocks, one
-// global atomic max per block column element.
+// Column exponents of B: one warp per block row, one block at a time.  For
+// bj <= 32 lane l keeps the max of element column l % bj over the rows
+// l / bj, l / bj + 32 / bj, ...; the lanes of one column merge through a
+// shared-memory atomic max, then one global atomic max per column element.
 __global__ void k_col_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                           const int8_t* __restrict__ col_bs, const double* __restrict__ d,
                           const int64_t* __restrict__ ebase, int* __restrict__ eb) {
-  const int lane = threadIdx.x & 31;
+  __shared__ unsigned long long cm[8][128];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
     const int bk = row_bs[r];
-    for (int64_t b = row_p[r] + lane; b < row_p[r + 1]; b += 32) {
+    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
       const int j = col[b], bj = col_bs[j];
       const double* x = d + off[b];
-      for (int c = 0; c < bj; ++c) {
-        double m = 0.0;
-        for (int kk = 0; kk < bk; ++kk) m = fmax(m, fabs(x[(int64_t)c * bk + kk]));
+      for (int c = lane; c < bj; c += 32) cm[wl][c] = 0ull;
+      __syncwarp();
+      if (bj <= 32) {
+        const int H = 32 / bj, c = lane % bj, h = lane / bj;
+        if (h < H) {
+          double m = 0.0;
+          for (int kr = h; kr < bk; kr += H) m = fmax(m, fabs(x[kr + c * bk]));
+          atomicMax(&cm[wl][c], (unsigned long long)__double_as_longlong(m));
+        }
+      } else {
+        Walk w(bj, lane);
+        for (int e = lane; e < bk * bj; e += 32, w.next())
+          atomicMax(&cm[wl][w.minor], (unsigned long long)__double_as_longlong(fabs(x[w.major + w.minor * bk])));
+      }
+      __syncwarp();
+      for (int c = lane; c < bj; c += 32) {
         int e = 0;
-        frexp(m, &e);
+        frexp(__longlong_as_double((long long)cm[wl][c]), &e);
         atomicMax(&eb[ebase[j] + c], e);
       }
+      __syncwarp();
     }
   }
 }

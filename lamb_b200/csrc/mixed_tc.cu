@@ -799,8 +799,16 @@ __device__ __forceinline__ void put_digits(int8_t* __restrict__ pan, int64_t pla
   }
 }
 
+// x * 2^-e: an exact power-of-two multiply where 2^-e is a normal double
+// (the result rounds once either way), ldexp outside that range.
+__device__ __forceinline__ double scale_down(double x, int e) {
+  return e > -1000 && e < 1000 ? x * __longlong_as_double((long long)(1023 - e) << 52) : ldexp(x, -e);
+}
+
 // A panels: element (pe, kc) of block (i, k) goes to panel row
-// base[I] + row(I, k) + kc, byte roff[i] + pe of that 128-byte row.
+// base[I] + row(I, k) + kc, byte roff[i] + pe of that 128-byte row.  Lanes
+// walk the block in storage order (pe fastest), so they write consecutive
+// bytes of a panel row.
 __global__ void k_tc_digits_a(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                               const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                               const int8_t* __restrict__ kbs, const double* __restrict__ data,
@@ -818,16 +826,17 @@ __global__ void k_tc_digits_a(int32_t n_rows, const int64_t* __restrict__ row_p,
       if (lane == 0) prow = base[I] + panel_row(bm, wrow, kbs, I, W, k);
       prow = __shfl_sync(0xffffffffu, prow, 0);
       const double* x = data + off[b];
-      for (int e = lane; e < bi * bk; e += 32) {
-        const int pe = e % bi, kc = e / bi;
-        put_digits(pan, plane, (prow + kc) * 128 + m0 + pe, ldexp(x[e], -ea[e0 + pe]));
-      }
+      Walk w(bi, lane);
+      for (int e = lane; e < bi * bk; e += 32, w.next())
+        put_digits(pan, plane, (prow + w.major) * 128 + m0 + w.minor, scale_down(x[e], ea[e0 + w.minor]));
     }
   }
 }
 
 // B panels: element (kr, q) of block (k, j) goes to panel row
-// base[J] + row(J, k) + kr, byte coff[j] + q of that 64-byte row.
+// base[J] + row(J, k) + kr, byte coff[j] + q of that 64-byte row.  Lanes
+// walk the block row by row (q fastest), so they write consecutive bytes of
+// a panel row (the strided reads stay within the block).
 __global__ void k_tc_digits_b(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                               const int64_t* __restrict__ off, const int8_t* __restrict__ kbs,
                               const int8_t* __restrict__ col_bs, const double* __restrict__ data,
@@ -845,9 +854,10 @@ __global__ void k_tc_digits_b(int32_t n_rows, const int64_t* __restrict__ row_p,
       prow = __shfl_sync(0xffffffffu, prow, 0);
       const double* x = data + off[b];
       const int64_t e0 = cbase[j];
-      for (int e = lane; e < bk * bj; e += 32) {
-        const int kr = e % bk, q = e / bk;
-        put_digits(pan, plane, (prow + kr) * 64 + n0 + q, ldexp(x[e], -eb[e0 + q]));
+      Walk w(bj, lane);
+      for (int e = lane; e < bk * bj; e += 32, w.next()) {
+        const int q = w.minor, kr = w.major;
+        put_digits(pan, plane, (prow + kr) * 64 + n0 + q, scale_down(x[kr + q * bk], eb[e0 + q]));
       }
     }
   }
@@ -950,6 +960,28 @@ __global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int
         rows[t] = nrows;
       }
     }
+  }
+}
+
+// Largest inner-atom count and K of any tile, and the pipeline stages of
+// all tiles (ceil(K / 32), at least one), into out[0..2].
+__global__ void k_tc_tile_stats(int64_t n_tiles, const int64_t* __restrict__ cnt, const int32_t* __restrict__ rows,
+                                unsigned long long* __restrict__ out) {
+  long long me = 0, mr = 0, st = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles; t += (int64_t)gridDim.x * blockDim.x) {
+    me = max(me, (long long)cnt[t]);
+    mr = max(mr, (long long)rows[t]);
+    st += rows[t] > 0 ? (rows[t] + kK - 1) / kK : 1;
+  }
+  for (int o = 16; o; o >>= 1) {
+    me = max(me, __shfl_xor_sync(0xffffffffu, me, o));
+    mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    st += __shfl_xor_sync(0xffffffffu, st, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&out[0], (unsigned long long)me);
+    atomicMax(&out[1], (unsigned long long)mr);
+    atomicAdd(&out[2], (unsigned long long)st);
   }
 }
 
@@ -1110,10 +1142,22 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, tra, basea, rc.n + 1));
   LAMB_TRY(exclusive_scan_i64(ctx, trb, baseb, cc.n + 1));
-  int64_t ra = 0, rb = 0;
-  LAMB_CUDA(ctx, cudaMemcpyAsync(&ra, basea + rc.n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  LAMB_CUDA(ctx, cudaMemcpyAsync(&rb, baseb + cc.n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  // ---- tiles: cluster pairs holding a C block ----
+  const int64_t n_map = (int64_t)rc.n * cc.n;
+  int64_t *flag, *pos;
+  LAMB_TRY(m.alloc(&flag, n_map + 1)); LAMB_TRY(m.alloc(&pos, n_map + 1));
+  LAMB_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int64_t) * (size_t)(n_map + 1), ctx->stream));
+  k_tc_tile_flags<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, d_rcl, d_ccl,
+                                                                         cc.n, flag);
+  LAMB_LAUNCHED(ctx);
+  LAMB_TRY(exclusive_scan_i64(ctx, flag, pos, n_map + 1));
+  // panel rows of A and B and the tile count in one read-back
+  int64_t h_sizes[3] = {0, 0, 0};
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&h_sizes[0], basea + rc.n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&h_sizes[1], baseb + cc.n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaMemcpyAsync(&h_sizes[2], pos + n_map, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
   LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int64_t ra = h_sizes[0], rb = h_sizes[1], n_tiles = h_sizes[2];
   if (ra + 1 > kRowMask || rb + 1 > INT_MAX) return LAMB_GPU_OK;  // panel rows beyond the entry format: not run
   // ---- digit panels (one zero row at the end of each plane for padding reads) ----
   const int64_t plane_a = ((ra + 1) * 128 + 255) & ~255ll, plane_b = ((rb + 1) * 64 + 255) & ~255ll;
@@ -1130,18 +1174,7 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
       B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, d_ccl, d_coff, W, bmb, wrb, baseb, mp.cbase,
       mp.eb, plane_b, pan_b);
   LAMB_LAUNCHED(ctx);
-  // ---- tiles ----
-  const int64_t n_map = (int64_t)rc.n * cc.n;
-  int64_t *flag, *pos;
-  LAMB_TRY(m.alloc(&flag, n_map + 1)); LAMB_TRY(m.alloc(&pos, n_map + 1));
-  LAMB_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(int64_t) * (size_t)(n_map + 1), ctx->stream));
-  k_tc_tile_flags<<<grid_for(32ll * C->n_rows, 256), 256, 0, ctx->stream>>>(C->n_rows, C->row_p, C->col, d_rcl, d_ccl,
-                                                                         cc.n, flag);
-  LAMB_LAUNCHED(ctx);
-  LAMB_TRY(exclusive_scan_i64(ctx, flag, pos, n_map + 1));
-  int64_t n_tiles = 0;
-  LAMB_CUDA(ctx, cudaMemcpyAsync(&n_tiles, pos + n_map, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // ---- tile list, C block lists, inner lists ----
   int2* tiles;
   int32_t* krows;
   int64_t *ecnt, *ebase, *lcnt, *lbase;
@@ -1171,20 +1204,18 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
       n_tiles, tiles, W, bma, bmb, wra, wrb, basea, baseb, A->col_bs, ecnt, krows, nullptr, nullptr);
   LAMB_LAUNCHED(ctx);
   LAMB_TRY(exclusive_scan_i64(ctx, ecnt, ebase, n_tiles + 1));
-  int64_t n_ent = 0, max_ent = 0, max_rows = 0;
-  LAMB_CUDA(ctx, cudaMemcpyAsync(&n_ent, ebase + n_tiles, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  LAMB_TRY(max_i64(ctx, ecnt, n_tiles, &max_ent));
-  {
-    std::vector<int32_t> h(n_tiles);
-    LAMB_CUDA(ctx, cudaMemcpyAsync(h.data(), krows, sizeof(int32_t) * (size_t)n_tiles, cudaMemcpyDeviceToHost, ctx->stream));
-    LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    double steps = 0.0;
-    for (int32_t x : h) {
-      max_rows = std::max<int64_t>(max_rows, x);
-      steps += x > 0 ? (x + kK - 1) / kK : 1;
-    }
-    *tensor_ops = steps * (kS * (kS + 1) / 2) * 2.0 * kM * kN * kK;
-  }
+  // {largest entry count, largest K, stages, entries} in one read-back
+  unsigned long long* d_stats;
+  LAMB_TRY(m.alloc(&d_stats, 4));
+  LAMB_CUDA(ctx, cudaMemsetAsync(d_stats, 0, 4 * sizeof(unsigned long long), ctx->stream));
+  k_tc_tile_stats<<<grid_for(n_tiles, 256), 256, 0, ctx->stream>>>(n_tiles, ecnt, krows, d_stats);
+  LAMB_LAUNCHED(ctx);
+  LAMB_CUDA(ctx, cudaMemcpyAsync(d_stats + 3, ebase + n_tiles, sizeof(int64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  unsigned long long h_stats[4] = {0, 0, 0, 0};
+  LAMB_CUDA(ctx, cudaMemcpyAsync(h_stats, d_stats, sizeof(h_stats), cudaMemcpyDeviceToHost, ctx->stream));
+  LAMB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int64_t max_ent = (int64_t)h_stats[0], max_rows = (int64_t)h_stats[1], n_ent = (int64_t)h_stats[3];
+  *tensor_ops = (double)h_stats[2] * (kS * (kS + 1) / 2) * 2.0 * kM * kN * kK;
   if (max_ent > kMaxEnt || max_rows > kMaxKRows) return LAMB_GPU_OK;  // outside the kernel's limits: not run
   uint2* ent;
   LAMB_TRY(m.alloc(&ent, n_ent));
@@ -1225,10 +1256,12 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
 namespace lamb {
 namespace tc {
 
-// One CTA per SM: lane 0 of warp 0 issues `iters` rounds of S(S+1)/2
-// tcgen05.mma kind::i8 (M = 128, N = n_dim, K = 32, operands from one zeroed
-// shared-memory stage, the same descriptors as the tile kernel for N = 64),
-// then waits for their completion (bounded).
+// One CTA per SM: lane 0 of warp 0 issues `iters` rounds of tcgen05.mma
+// kind::i8 (M = 128, K = 32, operands from one zeroed shared-memory stage),
+// then waits for their completion (bounded).  N = 64 or 256: S(S+1)/2 MMAs
+// of that width a round.  N = 0: the tile kernel's stage, the same nine
+// MMAs (one per A digit plane and run of up to four B digit planes, N = 64
+// to 256) with the same descriptors.
 template <int N>
 __global__ void __launch_bounds__(128, 1) k_tc_probe(int iters, int* err) {
   extern __shared__ unsigned char smem_raw[];
@@ -1240,7 +1273,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_probe(int iters, int* err) {
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = threadIdx.x; i < (kStageA + N * kK * kS) / 16; i += blockDim.x)
+  for (int i = threadIdx.x; i < (N == 0 ? kStageBytes : kStageA + N * kK * kS) / 16; i += blockDim.x)
     reinterpret_cast<int4*>(base)[i] = make_int4(0, 0, 0, 0);
   if (threadIdx.x == 0) {
     bar_init(&bar, 1);
@@ -1266,6 +1299,19 @@ __global__ void __launch_bounds__(128, 1) k_tc_probe(int iters, int* err) {
       // B rows of N bytes: 64-byte swizzle for N = 64, 128-byte for N >= 128 (one atom of 128 per 128 columns)
       const uint32_t bsw = N == 64 ? 4u : 2u, bsbo = N == 64 ? 512u : 1024u, blbo = N == 64 ? 64u : 4096u;
       const int levels = N <= 64 ? kS : 2;  // 512 tensor-memory columns hold 512 / N accumulators
+      if (N == 0) {
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+          for (int p = 0; p < kS; ++p) {
+            const uint64_t da = smem_desc(sa + p * kPlaneA, 128, 1024, 2);
+#pragma unroll
+            for (int q0 = 0; q0 < kS - p; q0 += 4) {
+              const int nq = (kS - p - q0) < 4 ? (kS - p - q0) : 4;
+              const uint64_t db = smem_desc(sb + q0 * kPlaneB, kPlaneB, 512, 4);
+              mma_i8(tmem + (uint32_t)(64 * (p + q0)), da, db, idesc_i8(64 * nq), 1u);
+            }
+          }
+      } else
       for (int it = 0; it < iters; ++it)
         for (int L = 0; L < kS; ++L)
           for (int p = 0; p <= L; ++p) {
@@ -1301,7 +1347,7 @@ static int32_t probe_n(int device, int reps, double* tops) {
   if (cudaSetDevice(device) != cudaSuccess) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  const size_t smem = (size_t)kStageA + (size_t)N * kK * kS + 1024;
+  const size_t smem = (N == 0 ? (size_t)kStageBytes : (size_t)kStageA + (size_t)N * kK * kS) + 1024;
   if (cudaFuncSetAttribute(k_tc_probe<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
   int* err = nullptr;
@@ -1328,7 +1374,7 @@ static int32_t probe_n(int device, int reps, double* tops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (ce != cudaSuccess || h_err) return make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_EXTERNAL_ERROR);
-  const double ops = 2.0 * kM * N * kK * (kS * (kS + 1) / 2) * (double)iters * sms;
+  const double ops = 2.0 * kM * (N == 0 ? kN : N) * kK * (kS * (kS + 1) / 2) * (double)iters * sms;
   *tops = ops / (best * 1e-3) / 1e12;
   return LAMB_GPU_OK;
 }
@@ -1337,9 +1383,11 @@ static int32_t probe_n(int device, int reps, double* tops) {
 }  // namespace lamb
 
 // int8 tensor-core throughput of tcgen05.mma kind::i8, M = 128, K = 32, for
-// N = 64 (the tile kernel's shape) or N = 256 (the widest instruction).
+// N = 64, N = 256 (the widest instruction), or n = 0: the tile kernel's
+// stage of nine MMAs of N = 64 to 256.
 extern "C" int32_t lamb_probe_int8_tcgen05_tops(int32_t device, int32_t n, int32_t reps, double* tops) {
   if (!tops) return lamb::make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
+  if (n == 0) return lamb::tc::probe_n<0>(device, reps, tops);
   if (n == 64) return lamb::tc::probe_n<64>(device, reps, tops);
   if (n == 256) return lamb::tc::probe_n<256>(device, reps, tops);
   return lamb::make_status(LAMB_LEVEL_FAILURE, LAMB_TYPE_WRONG_ARGS);
