@@ -72,6 +72,7 @@ __global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, con
         for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
           const int bk = col_bs[col[b]];
           const double* x = d + off[b];
+#pragma unroll 4
           for (int kc = g; kc < bk; kc += G) m = fmax(m, fabs(x[pe + kc * bi]));
         }
       if (g < G) atomicMax(&pm[wl][pe], (unsigned long long)__double_as_longlong(m));
@@ -116,6 +117,7 @@ __global__ void k_col_exp(int32_t n_rows, const int64_t* __restrict__ row_p, con
         const int H = 32 / bj, c = lane % bj, h = lane / bj;
         if (h < H) {
           double m = 0.0;
+#pragma unroll 4
           for (int kr = h; kr < bk; kr += H) m = fmax(m, fabs(x[kr + c * bk]));
           atomicMax(&cm[wl][c], (unsigned long long)__double_as_longlong(m));
         }

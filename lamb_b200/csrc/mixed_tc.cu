@@ -773,18 +773,16 @@ __global__ void k_tc_word_prefix(int32_t n_cl, int32_t W, const uint32_t* __rest
   }
 }
 
-// Panel row of inner atom k within cluster c's panel (relative to its base).
-__device__ __forceinline__ int64_t panel_row(const uint32_t* __restrict__ bm, const int32_t* __restrict__ wrow,
-                                             const int8_t* __restrict__ kbs, int64_t c, int32_t W, int k) {
+// Panel row of inner atom k within cluster c's panel (relative to its
+// base), by the whole warp: lane b adds the rows of atom 32 (k / 32) + b
+// when its bit is set and below k's.
+__device__ __forceinline__ int64_t panel_row_warp(const uint32_t* __restrict__ bm, const int32_t* __restrict__ wrow,
+                                                  const int8_t* __restrict__ kbs, int64_t c, int32_t W, int k,
+                                                  int lane) {
   const int w = k >> 5;
-  uint32_t below = bm[c * W + w] & ((1u << (k & 31)) - 1u);
-  int64_t r = wrow[c * W + w];
-  while (below) {
-    const int bit = __ffs(below) - 1;
-    below &= below - 1u;
-    r += kbs[32 * w + bit];
-  }
-  return r;
+  const uint32_t word = bm[c * W + w];
+  const int add = lane < (k & 31) && ((word >> lane) & 1u) ? kbs[32 * w + lane] : 0;
+  return wrow[c * W + w] + __reduce_add_sync(0xffffffffu, add);
 }
 
 // Writes the S digits of x (|x| < 1) to S planes: |127 x| < 127 and every
@@ -822,9 +820,7 @@ __global__ void k_tc_digits_a(int32_t n_rows, const int64_t* __restrict__ row_p,
     const int64_t e0 = rbase[i];
     for (int64_t b = row_p[i]; b < row_p[i + 1]; ++b) {
       const int k = col[b], bk = kbs[k];
-      int64_t prow = 0;
-      if (lane == 0) prow = base[I] + panel_row(bm, wrow, kbs, I, W, k);
-      prow = __shfl_sync(0xffffffffu, prow, 0);
+      const int64_t prow = base[I] + panel_row_warp(bm, wrow, kbs, I, W, k, lane);
       const double* x = data + off[b];
       Walk w(bi, lane);
       for (int e = lane; e < bi * bk; e += 32, w.next())
@@ -849,9 +845,7 @@ __global__ void k_tc_digits_b(int32_t n_rows, const int64_t* __restrict__ row_p,
     const int bk = kbs[k];
     for (int64_t b = row_p[k]; b < row_p[k + 1]; ++b) {
       const int j = col[b], J = ccl[j], n0 = coff[j], bj = col_bs[j];
-      int64_t prow = 0;
-      if (lane == 0) prow = base[J] + panel_row(bm, wrow, kbs, J, W, (int)k);
-      prow = __shfl_sync(0xffffffffu, prow, 0);
+      const int64_t prow = base[J] + panel_row_warp(bm, wrow, kbs, J, W, (int)k, lane);
       const double* x = data + off[b];
       const int64_t e0 = cbase[j];
       Walk w(bj, lane);
@@ -939,14 +933,19 @@ __global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int
       if (FILL) {
         const int incl = warp_incl_scan(c, lane);
         int64_t p = carry + incl - c;
-        while (x) {
-          const int bit = __ffs(x) - 1;
-          x &= x - 1u;
-          const int k = 32 * w + bit, bk = kbs[k];
-          if (bk == 0) continue;
-          const int64_t ar = basea[I] + panel_row(bma, wra, kbs, I, W, k);
-          const int64_t br = baseb[J] + panel_row(bmb, wrb, kbs, J, W, k);
-          ent[p++] = make_uint2((uint32_t)ar | ((uint32_t)bk << 25), (uint32_t)br);
+        if (x) {
+          // panel rows of A (cluster I) and B (cluster J): running sums over
+          // the set bits of each cluster's word, in increasing order
+          int64_t ar = basea[I] + wra[I * W + w], br = baseb[J] + wrb[J * W + w];
+          for (uint32_t y = xa | xb; y;) {
+            const int bit = __ffs(y) - 1;
+            y &= y - 1u;
+            const uint32_t mb = 1u << bit;
+            const int bk = kbs[32 * w + bit];
+            if ((x & mb) && bk > 0) ent[p++] = make_uint2((uint32_t)ar | ((uint32_t)bk << 25), (uint32_t)br);
+            if (xa & mb) ar += bk;
+            if (xb & mb) br += bk;
+          }
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
       } else {
