@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="water6144_cut8",
-                   choices=["water6144_cut8", "water1536_cut7", "water192_cut6", "batch64", "mcweeny384",
+                   choices=["water6144_cut8", "water1536_cut7", "water768_cut7", "water192_cut6", "batch64", "mcweeny384",
                             "adjoint96"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
@@ -61,7 +61,8 @@ def parse():
 
 def workload(name):
     from lamb_b200 import gen
-    return {"water6144_cut8": gen.WATER_6144, "water1536_cut7": gen.WATER_1536, "water192_cut6": gen.WATER_192}[name]
+    return {"water6144_cut8": gen.WATER_6144, "water1536_cut7": gen.WATER_1536, "water768_cut7": gen.WATER_768,
+            "water192_cut6": gen.WATER_192}[name]
 
 
 def workload_config(wl, g) -> dict:
@@ -297,6 +298,9 @@ def run_mixed_leg(ctx, lib, local, da, db, dc, wl, args, flops, ms_fp64):
                            "peak_source": "tcgen05 kind::i8 probe issuing the tile kernel's own nine-MMA stage "
                                           "(lamb_probe_int8_tcgen05_tops n=0) on this GPU in this run",
                            "tensor_ops_per_multiply": t_ops,
+                           "traffic": committed_traffic("k_tc_tiles", wl.name),
+                           "traffic_scope": "DRAM bytes of the multiply's tile-kernel launch, scaled by tensor ops "
+                                            "from the committed small-case capture; null when none",
                            "useful_fraction": flops * s_m * (s_m + 1) / 2 / t_ops,
                            "note": "executed ops include the zero padding of the cluster tiles; useful_fraction = "
                                    "FP64-equivalent flops x 21 digit pairs / executed ops"}

@@ -129,6 +129,9 @@ WATER_192 = WaterWorkload("water192_cut6", 192, 17.9, 6.0, 1e-8, 0, 0, 0)
 WATER_6144 = WaterWorkload("water6144_cut8", 6144, 56.8, 8.0, 1e-10, 1, 1, 2)
 # 1536 waters at the same density, cutoff 7 A, seed 4 (the purification-adjoint geometry).
 WATER_1536 = WaterWorkload("water1536_cut7", 1536, box_side(1536), 7.0, 1e-10, 4, 4, 5)
+# A profiling size of the same family: small enough for multi-pass ncu
+# captures (a few GB on the device), larger than L2.
+WATER_768 = WaterWorkload("water768_cut7", 768, box_side(768), 7.0, 1e-10, 11, 11, 12)
 
 
 def batch_instances(n: int = 64, seed: int = 3, mol_range=(96, 1536), cut_range=(5.0, 9.0)):
