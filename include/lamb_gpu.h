@@ -143,6 +143,10 @@ typedef struct lamb_gpu_mult_stats {
   double tensor_ops;         /* mixed, tensor-core path: int8 multiply-add ops
                                 the tile kernel executed (2 per MAC, padding
                                 of the cluster tiles included); else 0       */
+  double ms_kernel;          /* device time of the product kernel's launches
+                                alone: FP64, the k_stacked launches of all row
+                                chunks (without the chunks' stack fills);
+                                mixed, the numeric phase                      */
 } lamb_gpu_mult_stats;
 
 typedef struct lamb_gpu_ctx lamb_gpu_ctx;

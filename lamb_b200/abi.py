@@ -37,6 +37,7 @@ class MultStats(C.Structure):
         ("flops", C.c_double), ("ms_symbolic", C.c_double), ("ms_numeric", C.c_double), ("ms_total", C.c_double),
         ("mixed_slices", C.c_int32), ("kernel_launches", C.c_int32),
         ("ms_prepare", C.c_double), ("ms_filter", C.c_double), ("tensor_ops", C.c_double),
+        ("ms_kernel", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -100,6 +100,9 @@ struct Ctx {
   // Chunked numeric phase of the last multiply (downloads overlap it).
   DevMatrix* chunk_m = nullptr;
   cudaEvent_t chunk_ev[kMaxChunks] = {};
+  // timing events around each row chunk's product-kernel launch (FP64 path)
+  cudaEvent_t kern_ev[2][kMaxChunks] = {};
+  int kern_chunks = 0;
   cudaStream_t copy_stream = nullptr;
 };
 

@@ -628,6 +628,8 @@ int32_t lamb_gpu_ctx_create(int32_t device, lamb_gpu_ctx** out) {
   }
   for (auto& ev : ctx->ev) cudaEventCreate(&ev);
   for (auto& ev : ctx->chunk_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  for (auto& row : ctx->kern_ev)
+    for (auto& ev : row) cudaEventCreate(&ev);
   cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
   if (const char* t = std::getenv("LAMB_GPU_TRACE")) {
     ctx->trace = t[0] == '1' || t[0] == '2';
@@ -654,6 +656,8 @@ int32_t lamb_gpu_ctx_destroy(lamb_gpu_ctx* c) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& ev : ctx->ev) cudaEventDestroy(ev);
   for (auto& ev : ctx->chunk_ev) cudaEventDestroy(ev);
+  for (auto& row : ctx->kern_ev)
+    for (auto& ev : row) cudaEventDestroy(ev);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->pend_ev) cudaEventDestroy(ctx->pend_ev);
   if (ctx->pend_h) cudaFreeHost(ctx->pend_h);

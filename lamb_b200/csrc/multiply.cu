@@ -791,9 +791,14 @@ static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C
   // the chunk's work items: row lengths in processing order, their scan, the items
   k_order_lens<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, A->order, C->row_p, d_len);
   LAMB_LAUNCHED(ctx);
+  ctx->kern_chunks = P;
   for (int p = 0; p < P; ++p) {
     const int nr = q[p + 1] - q[p];
-    if (nr == 0) continue;
+    if (nr == 0) {
+      LAMB_CUDA(ctx, cudaEventRecord(ctx->kern_ev[0][p], ctx->stream));
+      LAMB_CUDA(ctx, cudaEventRecord(ctx->kern_ev[1][p], ctx->stream));
+      continue;
+    }
     fill<<<std::min(fgrid_all, nr), kSymThreads, sym.fill_smem, ctx->stream>>>(
         nr, A->row_p, A->col, A->norms, B->row_p, B->col, B->norms, sym.fill_eps, sym.fill_n_words, sym.fill_na_max,
         sym.fill_nc_max, C->row_p, d_rel + q[p], C->col, sym.stack_p, a_offk, B->off, ent, nullptr, A->order + q[p],
@@ -804,8 +809,10 @@ static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C
                                                                  C->off, C->row_bs, C->col_bs, sym.stack_p,
                                                                  work + item[p], work_c + item[p], d_end + q[p]);
     LAMB_LAUNCHED(ctx);
+    LAMB_CUDA(ctx, cudaEventRecord(ctx->kern_ev[0][p], ctx->stream));
     LAMB_TRY(run_stacked(ctx, item[p + 1] - item[p], work + item[p], work_c + item[p], ent, A->data, B->data,
                          C->data, c_nrm, false, false, mi));
+    LAMB_CUDA(ctx, cudaEventRecord(ctx->kern_ev[1][p], ctx->stream));
     LAMB_CUDA(ctx, cudaEventRecord(ctx->chunk_ev[p], ctx->stream));
   }
   if (layout_ok) {
@@ -829,6 +836,7 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
   lamb_gpu_mult_stats st{};
   const int64_t launches0 = ctx->launches;
   if (timed) LAMB_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+  ctx->kern_chunks = 0;
   Symbolic sym;
   int64_t* a_offk = nullptr;
   double* c_nrm = nullptr;
@@ -945,6 +953,16 @@ int32_t multiply_impl(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, double
     st.ms_total = t03;
     st.ms_filter = t23;
     st.ms_prepare = t04;
+    st.ms_kernel = t12;  // the numeric phase is the product kernel, except in the FP64 row chunks:
+    if (!mixed && ctx->kern_chunks > 0) {
+      double s = 0.0;
+      for (int p = 0; p < ctx->kern_chunks; ++p) {
+        float e = 0.f;
+        cudaEventElapsedTime(&e, ctx->kern_ev[0][p], ctx->kern_ev[1][p]);
+        s += e;
+      }
+      st.ms_kernel = s;
+    }
   }
   ctx->last_stats = st;
   if (stats) *stats = st;

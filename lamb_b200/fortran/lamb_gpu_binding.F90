@@ -37,7 +37,7 @@ module lamb_gpu_bindings
      integer(c_int64_t) :: n_products, n_products_skipped, n_c_blocks, n_c_blocks_dropped
      real(c_double) :: flops, ms_symbolic, ms_numeric, ms_total
      integer(c_int32_t) :: mixed_slices, kernel_launches
-     real(c_double) :: ms_prepare, ms_filter, tensor_ops
+     real(c_double) :: ms_prepare, ms_filter, tensor_ops, ms_kernel
   end type lamb_gpu_mult_stats
 
   public :: lamb_gpu_ctx_create, lamb_gpu_ctx_destroy, lamb_gpu_last_error, lamb_gpu_status_level, &
