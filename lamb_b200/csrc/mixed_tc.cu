@@ -905,8 +905,52 @@ __global__ void k_tc_tile_blocks(int32_t n_rows, const int64_t* __restrict__ row
 }
 
 // Inner atoms of every tile: k with A_ik for some i in I and B_kj for some j
-// in J (and b_k > 0).  Count pass: entries and panel rows per tile.  Fill
-// pass: (A panel row | b_k << 25, B panel row) per entry.  One warp per tile.
+// in J (and b_k > 0), in increasing k.  Consecutive such atoms whose panel
+// rows follow on in both panels (no atom of only one cluster between them)
+// merge into one entry of up to 127 rows, within one 32-atom bitmap word.
+// Count pass: entries and panel rows per tile.  Fill pass: (A panel row |
+// rows << 25, B panel row) per entry.  One warp per tile, a lane per word.
+template <bool FILL>
+__device__ __forceinline__ int tile_word_entries(uint32_t xa, uint32_t xb, int w, const int8_t* __restrict__ kbs,
+                                                 int64_t ar, int64_t br, uint2* __restrict__ out, int* nrows) {
+  const uint32_t x = xa & xb;
+  int n = 0, open = 0;  // rows of the open entry (0: none)
+  int64_t oa = 0, ob = 0;
+  for (uint32_t y = xa | xb; y;) {
+    const int bit = __ffs(y) - 1;
+    y &= y - 1u;
+    const uint32_t mb = 1u << bit;
+    const int bk = kbs[32 * w + bit];
+    if (bk > 0) {
+      if (x & mb) {
+        *nrows += bk;
+        if (open > 0 && open + bk <= 127) {
+          open += bk;
+        } else {
+          if (open > 0) {
+            if (FILL) out[n] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
+            ++n;
+          }
+          oa = ar;
+          ob = br;
+          open = bk;
+        }
+      } else if (open > 0) {  // rows of one panel only: the next entry starts apart
+        if (FILL) out[n] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
+        ++n;
+        open = 0;
+      }
+    }
+    if (xa & mb) ar += bk;
+    if (xb & mb) br += bk;
+  }
+  if (open > 0) {
+    if (FILL) out[n] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
+    ++n;
+  }
+  return n;
+}
+
 template <bool FILL>
 __global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int32_t W,
                             const uint32_t* __restrict__ bma, const uint32_t* __restrict__ bmb,
@@ -922,30 +966,24 @@ __global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int
     for (int w0 = 0; w0 < W; w0 += 32) {
       const int w = w0 + lane;
       const uint32_t xa = w < W ? bma[I * W + w] : 0u, xb = w < W ? bmb[J * W + w] : 0u;
-      uint32_t x = xa & xb;
       int c = 0;
-      for (uint32_t y = x; y;) {
-        const int bit = __ffs(y) - 1;
-        y &= y - 1u;
-        const int bk = kbs[32 * w + bit];
-        if (bk > 0) { ++c; nrows += bk; }
+      if (xa & xb) {
+        const int64_t ar = basea[I] + wra[I * W + w], br = baseb[J] + wrb[J * W + w];
+        if (FILL) {
+          // entry positions need the count first: count, scan, then fill
+          int dummy = 0;
+          c = tile_word_entries<false>(xa, xb, w, kbs, ar, br, nullptr, &dummy);
+        } else {
+          c = tile_word_entries<false>(xa, xb, w, kbs, ar, br, nullptr, &nrows);
+        }
       }
       if (FILL) {
         const int incl = warp_incl_scan(c, lane);
-        int64_t p = carry + incl - c;
-        if (x) {
-          // panel rows of A (cluster I) and B (cluster J): running sums over
-          // the set bits of each cluster's word, in increasing order
-          int64_t ar = basea[I] + wra[I * W + w], br = baseb[J] + wrb[J * W + w];
-          for (uint32_t y = xa | xb; y;) {
-            const int bit = __ffs(y) - 1;
-            y &= y - 1u;
-            const uint32_t mb = 1u << bit;
-            const int bk = kbs[32 * w + bit];
-            if ((x & mb) && bk > 0) ent[p++] = make_uint2((uint32_t)ar | ((uint32_t)bk << 25), (uint32_t)br);
-            if (xa & mb) ar += bk;
-            if (xb & mb) br += bk;
-          }
+        const int64_t p = carry + incl - c;
+        if (c > 0) {
+          int dummy = 0;
+          tile_word_entries<true>(xa, xb, w, kbs, basea[I] + wra[I * W + w], baseb[J] + wrb[J * W + w], ent + p,
+                                  &dummy);
         }
         carry += __shfl_sync(0xffffffffu, incl, 31);
       } else {

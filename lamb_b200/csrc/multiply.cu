@@ -681,8 +681,17 @@ static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C
   if ((int)ord.size() != n || !A->order || (int)sym.h_row_ent.size() != n)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_INTERNAL_ERROR, "numeric: row order or row stacks missing");
   const bool layout_ok = (int64_t)C->h_order.size() == n && (int64_t)sym.h_base.size() == (int64_t)n * S;
+  // The fill runs one CTA per C row: a chunk gets at least as many rows as
+  // the fill keeps resident, so that it fills the GPU (few heavy rows, as in
+  // the products of dense density matrices, would otherwise leave most SMs idle).
+  auto fill = k_sym_fill<false>;
+  if (sym.fill_smem > 48 * 1024)
+    LAMB_CUDA(ctx, cudaFuncSetAttribute(fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym.fill_smem));
+  int fgrid_all = 1;
+  LAMB_TRY(resident_grid(ctx, fill, sym.fill_smem, n, &fgrid_all));
+  const int min_rows = std::max(1, fgrid_all);
   // ---- chunk boundaries (processing positions) ----
-  const int P0 = (layout_ok && sym.c_nnz >= 4 * kMinChunks) ? kMinChunks : 1;
+  const int P0 = (layout_ok && sym.c_nnz >= 4 * kMinChunks) ? std::max(1, std::min(kMinChunks, n / min_rows)) : 1;
   std::vector<int> q0(P0 + 1, n);
   q0[0] = 0;
   {
@@ -702,7 +711,7 @@ static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C
       int64_t ent = 0;
       for (int w = q0[p]; w < q0[p + 1]; ++w) {
         const int64_t re = sym.h_row_ent[ord[w]];
-        if (ent + re > cap && w > q.back()) {
+        if (ent + re > cap && w - q.back() >= min_rows) {
           q.push_back(w);
           ent = 0;
         }
@@ -783,11 +792,6 @@ static int32_t numeric_chunks(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C
   LAMB_TRY(dalloc(ctx, &d_cum, n));
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_rel, rel.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
   LAMB_CUDA(ctx, cudaMemcpyAsync(d_end, ends.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
-  auto fill = k_sym_fill<false>;
-  if (sym.fill_smem > 48 * 1024)
-    LAMB_CUDA(ctx, cudaFuncSetAttribute(fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym.fill_smem));
-  int fgrid_all = 1;
-  LAMB_TRY(resident_grid(ctx, fill, sym.fill_smem, n, &fgrid_all));
   // the chunk's work items: row lengths in processing order, their scan, the items
   k_order_lens<<<grid_for(n, 128), 128, 0, ctx->stream>>>(n, A->order, C->row_p, d_len);
   LAMB_LAUNCHED(ctx);
