@@ -48,67 +48,66 @@ constexpr int64_t kLevelInnerMax7 = (int64_t)INT_MAX / (7 * 64 * 64);
 __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
 // ---- scales ----------------------------------------------------------------------------
-// Row exponents of A: one warp per block row.  For bi <= 32 lane l keeps
-// the running max of element row l % bi over the columns l / bi, l / bi +
-// 32 / bi, ... of every block of the row (lanes of one column group read
-// consecutive elements); the lanes of one element row then merge through a
-// shared-memory atomic max (non-negative doubles order like their bit
-// patterns).  Larger blocks merge every element.
+// Row exponents of A: one CTA per block row, its warps taking every 8th
+// block of the row (memory parallelism across the row's blocks).  For
+// bi <= 32 lane l keeps the running max of element row l % bi over the
+// columns l / bi, l / bi + 32 / bi, ... of its blocks; all lanes of one
+// element row then merge through a shared-memory atomic max (non-negative
+// doubles order like their bit patterns).  Larger blocks merge every element.
 __global__ void k_row_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                           const int8_t* __restrict__ col_bs, const double* __restrict__ d,
                           const int64_t* __restrict__ ebase, int* __restrict__ ea) {
-  __shared__ unsigned long long pm[8][128];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
+  __shared__ unsigned long long pm[128];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5, nwl = blockDim.x >> 5;
+  for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
     const int bi = row_bs[r];
-    for (int p = lane; p < bi; p += 32) pm[wl][p] = 0ull;
-    __syncwarp();
+    for (int p = threadIdx.x; p < bi; p += blockDim.x) pm[p] = 0ull;
+    __syncthreads();
     if (bi <= 32) {
       const int G = 32 / bi, pe = lane % bi, g = lane / bi;
       double m = 0.0;
       if (g < G)
-        for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+        for (int64_t b = row_p[r] + wl; b < row_p[r + 1]; b += nwl) {
           const int bk = col_bs[col[b]];
           const double* x = d + off[b];
 #pragma unroll 4
           for (int kc = g; kc < bk; kc += G) m = fmax(m, fabs(x[pe + kc * bi]));
         }
-      if (g < G) atomicMax(&pm[wl][pe], (unsigned long long)__double_as_longlong(m));
+      if (g < G) atomicMax(&pm[pe], (unsigned long long)__double_as_longlong(m));
     } else {
-      for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+      for (int64_t b = row_p[r] + wl; b < row_p[r + 1]; b += nwl) {
         const int ne = bi * col_bs[col[b]];
         const double* x = d + off[b];
         Walk w(bi, lane);
         for (int e = lane; e < ne; e += 32, w.next())
-          atomicMax(&pm[wl][w.minor], (unsigned long long)__double_as_longlong(fabs(x[e])));
+          atomicMax(&pm[w.minor], (unsigned long long)__double_as_longlong(fabs(x[e])));
       }
     }
-    __syncwarp();
-    for (int p = lane; p < bi; p += 32) {
+    __syncthreads();
+    for (int p = threadIdx.x; p < bi; p += blockDim.x) {
       int e = 0;
-      frexp(__longlong_as_double((long long)pm[wl][p]), &e);
+      frexp(__longlong_as_double((long long)pm[p]), &e);
       ea[ebase[r] + p] = e;
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
-// Column exponents of B: one warp per block row, one block at a time.  For
-// bj <= 32 lane l keeps the max of element column l % bj over the rows
-// l / bj, l / bj + 32 / bj, ...; the lanes of one column merge through a
-// shared-memory atomic max, then one global atomic max per column element.
+// Column exponents of B: one CTA per block row, its warps taking every 8th
+// block of the row.  For bj <= 32 lane l keeps the max of element column
+// l % bj over the rows l / bj, l / bj + 32 / bj, ...; the lanes of one
+// column merge through a shared-memory atomic max, then one global atomic
+// max per block column element.
 __global__ void k_col_exp(int32_t n_rows, const int64_t* __restrict__ row_p, const int32_t* __restrict__ col,
                           const int64_t* __restrict__ off, const int8_t* __restrict__ row_bs,
                           const int8_t* __restrict__ col_bs, const double* __restrict__ d,
                           const int64_t* __restrict__ ebase, int* __restrict__ eb) {
   __shared__ unsigned long long cm[8][128];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_rows; r += nw) {
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5, nwl = blockDim.x >> 5;
+  for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
     const int bk = row_bs[r];
-    for (int64_t b = row_p[r]; b < row_p[r + 1]; ++b) {
+    for (int64_t b = row_p[r] + wl; b < row_p[r + 1]; b += nwl) {
       const int j = col[b], bj = col_bs[j];
       const double* x = d + off[b];
       for (int c = lane; c < bj; c += 32) cm[wl][c] = 0ull;
@@ -439,7 +438,7 @@ static std::vector<int64_t> elem_base(const std::vector<int8_t>& bs) {
 int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, MixedPlanes* mp, bool exps_only) {
   if (max_block(A->h_row_bs) > 127 || max_block(B->h_col_bs) > 127)
     return fail(ctx, LAMB_LEVEL_FAILURE, LAMB_TYPE_UNIMPLEMENTED, "mixed: block too large");
-  static_assert(kThreads <= 256, "k_row_exp keeps 8 warps x 128 rows of maxima in shared memory");
+  static_assert(kThreads <= 256, "k_col_exp keeps 8 warps x 128 columns of maxima in shared memory");
   mp->s = s;
   const auto ra = elem_base(A->h_row_bs), cbv = elem_base(B->h_col_bs);
   LAMB_TRY(dalloc(ctx, &mp->rbase, (int64_t)ra.size()));
@@ -451,12 +450,12 @@ int32_t build_slices(Ctx* ctx, const DevMatrix* A, const DevMatrix* B, int s, Mi
   // eb starts at 0x80808080 (byte fill), below any frexp exponent, for the atomic max
   LAMB_CUDA(ctx, cudaMemsetAsync(mp->eb, 0x80, sizeof(int) * std::max<int64_t>(cbv.back(), 1), ctx->stream));
   if (A->nnz) {
-    k_row_exp<<<grid_for((int64_t)A->n_rows * 32), kThreads, 0, ctx->stream>>>(
+    k_row_exp<<<grid_for((int64_t)A->n_rows * kThreads), kThreads, 0, ctx->stream>>>(
         A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, mp->rbase, mp->ea);
     LAMB_LAUNCHED(ctx);
   }
   if (B->nnz) {
-    k_col_exp<<<grid_for((int64_t)B->n_rows * 32), kThreads, 0, ctx->stream>>>(
+    k_col_exp<<<grid_for((int64_t)B->n_rows * kThreads), kThreads, 0, ctx->stream>>>(
         B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, mp->cbase, mp->eb);
     LAMB_LAUNCHED(ctx);
   }
