@@ -355,6 +355,27 @@ def test_mixed_tensor_core_error(gpu_ctx, n_mol, cutoff, blk_o, blk_h):
     assert err <= TOL_MIXED, err
 
 
+def test_mixed_tensor_core_dense_tiles(gpu_ctx):
+    """A dense product (352 waters, cutoff across the box): every tile couples
+    to all 1,056 inner atoms, more entries than the tile kernel holds unless
+    consecutive atoms merge into entries of contiguous panel rows.  The
+    tensor-core kernel must run (tensor_ops > 0) and match the FP64 product
+    within 1e-11."""
+    g = WaterGeometry(352, None, 30.0, seed=3)
+    a, b = g.matrix(1), g.matrix(2)
+    da, db = gpu_ctx.upload(a), gpu_ctx.upload(b)
+    da.set_positions(g.sector_positions(), g.box)
+    c64, cm = gpu_ctx.create_like(da), gpu_ctx.create_like(da)
+    st64 = gpu_ctx.multiply(da, db, c64, 1e-10)
+    stm = gpu_ctx.multiply(da, db, cm, 1e-10, gpu.MIXED)
+    assert stm["tensor_ops"] > 0
+    assert stm["n_c_blocks"] == st64["n_c_blocks"] == (3 * 352) ** 2
+    err = gpu_ctx.diff_frobenius(cm, c64) / gpu_ctx.frobenius(c64)
+    assert err <= TOL_MIXED, err
+    for m in (cm, c64, db, da):
+        m.destroy()
+
+
 def test_mixed_tensor_core_keeps_filtered_pattern(gpu_ctx):
     """With an eps that filters products, C's pattern is the filtered one
     (bit-exact with the oracle); its blocks carry every product, the
