@@ -912,7 +912,8 @@ __global__ void k_tc_tile_blocks(int32_t n_rows, const int64_t* __restrict__ row
 // rows << 25, B panel row) per entry.  One warp per tile, a lane per word.
 template <bool FILL>
 __device__ __forceinline__ int tile_word_entries(uint32_t xa, uint32_t xb, int w, const int8_t* __restrict__ kbs,
-                                                 int64_t ar, int64_t br, uint2* __restrict__ out, int* nrows) {
+                                                 int64_t ar, int64_t br, uint2* __restrict__ out, int* nrows,
+                                                 int* slot) {
   const uint32_t x = xa & xb;
   int n = 0, open = 0;  // rows of the open entry (0: none)
   int64_t oa = 0, ob = 0;
@@ -928,7 +929,7 @@ __device__ __forceinline__ int tile_word_entries(uint32_t xa, uint32_t xb, int w
           open += bk;
         } else {
           if (open > 0) {
-            if (FILL) out[n] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
+            if (FILL) out[atomicAdd(slot, 1)] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
             ++n;
           }
           oa = ar;
@@ -936,7 +937,7 @@ __device__ __forceinline__ int tile_word_entries(uint32_t xa, uint32_t xb, int w
           open = bk;
         }
       } else if (open > 0) {  // rows of one panel only: the next entry starts apart
-        if (FILL) out[n] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
+        if (FILL) out[atomicAdd(slot, 1)] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
         ++n;
         open = 0;
       }
@@ -945,50 +946,41 @@ __device__ __forceinline__ int tile_word_entries(uint32_t xa, uint32_t xb, int w
     if (xb & mb) br += bk;
   }
   if (open > 0) {
-    if (FILL) out[n] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
+    if (FILL) out[atomicAdd(slot, 1)] = make_uint2((uint32_t)oa | ((uint32_t)open << 25), (uint32_t)ob);
     ++n;
   }
   return n;
 }
 
 template <bool FILL>
-__global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int32_t W,
-                            const uint32_t* __restrict__ bma, const uint32_t* __restrict__ bmb,
-                            const int32_t* __restrict__ wra, const int32_t* __restrict__ wrb,
-                            const int64_t* __restrict__ basea, const int64_t* __restrict__ baseb,
-                            const int8_t* __restrict__ kbs, int64_t* __restrict__ cnt, int32_t* __restrict__ rows,
-                            const int64_t* __restrict__ ebase, uint2* __restrict__ ent) {
-  const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(256) k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int32_t W,
+                                                   const uint32_t* __restrict__ bma, const uint32_t* __restrict__ bmb,
+                                                   const int32_t* __restrict__ wra, const int32_t* __restrict__ wrb,
+                                                   const int64_t* __restrict__ basea, const int64_t* __restrict__ baseb,
+                                                   const int8_t* __restrict__ kbs, int64_t* __restrict__ cnt,
+                                                   int32_t* __restrict__ rows, const int64_t* __restrict__ ebase,
+                                                   uint2* __restrict__ ent) {
+  // Fill pass: entries take the next free slot of their tile (a per-warp
+  // counter); the K-row order inside a tile does not change the exact int32
+  // level sums, and the producers' row prefix follows the stored order.
+  __shared__ int slot[8];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   for (int64_t t = global_warp(); t < n_tiles; t += grid_warps()) {
     const int64_t I = tiles[t].x, J = tiles[t].y;
-    int64_t carry = FILL ? ebase[t] : 0;
+    int64_t carry = 0;
     int nrows = 0;
+    if (FILL && lane == 0) slot[wl] = 0;
+    __syncwarp();
+    uint2* out = FILL ? ent + ebase[t] : nullptr;
     for (int w0 = 0; w0 < W; w0 += 32) {
       const int w = w0 + lane;
       const uint32_t xa = w < W ? bma[I * W + w] : 0u, xb = w < W ? bmb[J * W + w] : 0u;
       int c = 0;
       if (xa & xb) {
         const int64_t ar = basea[I] + wra[I * W + w], br = baseb[J] + wrb[J * W + w];
-        if (FILL) {
-          // entry positions need the count first: count, scan, then fill
-          int dummy = 0;
-          c = tile_word_entries<false>(xa, xb, w, kbs, ar, br, nullptr, &dummy);
-        } else {
-          c = tile_word_entries<false>(xa, xb, w, kbs, ar, br, nullptr, &nrows);
-        }
+        c = tile_word_entries<FILL>(xa, xb, w, kbs, ar, br, out, &nrows, &slot[wl]);
       }
-      if (FILL) {
-        const int incl = warp_incl_scan(c, lane);
-        const int64_t p = carry + incl - c;
-        if (c > 0) {
-          int dummy = 0;
-          tile_word_entries<true>(xa, xb, w, kbs, basea[I] + wra[I * W + w], baseb[J] + wrb[J * W + w], ent + p,
-                                  &dummy);
-        }
-        carry += __shfl_sync(0xffffffffu, incl, 31);
-      } else {
-        carry += warp_sum_ll(c);
-      }
+      if (!FILL) carry += warp_sum_ll(c);
     }
     if (!FILL) {
       nrows = (int)warp_sum_ll(nrows);
@@ -997,6 +989,7 @@ __global__ void k_tc_tile_k(int64_t n_tiles, const int2* __restrict__ tiles, int
         rows[t] = nrows;
       }
     }
+    __syncwarp();
   }
 }
 
