@@ -803,6 +803,10 @@ __device__ __forceinline__ double scale_down(double x, int e) {
   return e > -1000 && e < 1000 ? x * __longlong_as_double((long long)(1023 - e) << 52) : ldexp(x, -e);
 }
 
+// Warps per block row in the digit kernels (memory parallelism across the
+// row's blocks).
+constexpr int kDigitWays = 8;
+
 // A panels: element (pe, kc) of block (i, k) goes to panel row
 // base[I] + row(I, k) + kc, byte roff[i] + pe of that 128-byte row.  Lanes
 // walk the block in storage order (pe fastest), so they write consecutive
@@ -815,10 +819,12 @@ __global__ void k_tc_digits_a(int32_t n_rows, const int64_t* __restrict__ row_p,
                               const int64_t* __restrict__ base, const int64_t* __restrict__ rbase,
                               const int* __restrict__ ea, int64_t plane, int8_t* __restrict__ pan) {
   const int lane = threadIdx.x & 31;
-  for (int64_t i = global_warp(); i < n_rows; i += grid_warps()) {
+  // kDigitWays warps per block row, each every kDigitWays-th block of it
+  for (int64_t gw = global_warp(); gw < (int64_t)n_rows * kDigitWays; gw += grid_warps()) {
+    const int64_t i = gw / kDigitWays;
     const int I = rcl[i], m0 = roff[i], bi = row_bs[i];
     const int64_t e0 = rbase[i];
-    for (int64_t b = row_p[i]; b < row_p[i + 1]; ++b) {
+    for (int64_t b = row_p[i] + gw % kDigitWays; b < row_p[i + 1]; b += kDigitWays) {
       const int k = col[b], bk = kbs[k];
       const int64_t prow = base[I] + panel_row_warp(bm, wrow, kbs, I, W, k, lane);
       const double* x = data + off[b];
@@ -841,9 +847,10 @@ __global__ void k_tc_digits_b(int32_t n_rows, const int64_t* __restrict__ row_p,
                               const int64_t* __restrict__ base, const int64_t* __restrict__ cbase,
                               const int* __restrict__ eb, int64_t plane, int8_t* __restrict__ pan) {
   const int lane = threadIdx.x & 31;
-  for (int64_t k = global_warp(); k < n_rows; k += grid_warps()) {
+  for (int64_t gw = global_warp(); gw < (int64_t)n_rows * kDigitWays; gw += grid_warps()) {
+    const int64_t k = gw / kDigitWays;
     const int bk = kbs[k];
-    for (int64_t b = row_p[k]; b < row_p[k + 1]; ++b) {
+    for (int64_t b = row_p[k] + gw % kDigitWays; b < row_p[k + 1]; b += kDigitWays) {
       const int j = col[b], J = ccl[j], n0 = coff[j], bj = col_bs[j];
       const int64_t prow = base[J] + panel_row_warp(bm, wrow, kbs, J, W, (int)k, lane);
       const double* x = data + off[b];
@@ -1196,11 +1203,11 @@ int32_t numeric_mixed_tc(Ctx* ctx, DevMatrix* A, DevMatrix* B, DevMatrix* C, con
   LAMB_TRY(scratch(ctx, kScrPlaneB, plane_b * kS, &pan_b));
   LAMB_CUDA(ctx, cudaMemsetAsync(pan_a, 0, (size_t)(plane_a * kS), ctx->stream));
   LAMB_CUDA(ctx, cudaMemsetAsync(pan_b, 0, (size_t)(plane_b * kS), ctx->stream));
-  k_tc_digits_a<<<grid_for(32ll * A->n_rows, 256), 256, 0, ctx->stream>>>(
+  k_tc_digits_a<<<grid_for(32ll * kDigitWays * A->n_rows, 256), 256, 0, ctx->stream>>>(
       A->n_rows, A->row_p, A->col, A->off, A->row_bs, A->col_bs, A->data, d_rcl, d_roff, W, bma, wra, basea, mp.rbase,
       mp.ea, plane_a, pan_a);
   LAMB_LAUNCHED(ctx);
-  k_tc_digits_b<<<grid_for(32ll * B->n_rows, 256), 256, 0, ctx->stream>>>(
+  k_tc_digits_b<<<grid_for(32ll * kDigitWays * B->n_rows, 256), 256, 0, ctx->stream>>>(
       B->n_rows, B->row_p, B->col, B->off, B->row_bs, B->col_bs, B->data, d_ccl, d_coff, W, bmb, wrb, baseb, mp.cbase,
       mp.eb, plane_b, pan_b);
   LAMB_LAUNCHED(ctx);
