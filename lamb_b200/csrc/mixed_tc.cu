@@ -71,7 +71,7 @@ constexpr int kPlaneB = kK * kN;
 constexpr int kStageA = kS * kPlaneA;
 constexpr int kStageB = kS * kPlaneB;
 constexpr int kStageBytes = kStageA + kStageB;  // 36,864: a multiple of 1,024
-constexpr int kMaxEnt = 1024;         // inner atoms of one tile
+constexpr int kMaxEnt = 1024;         // inner-list entries of one tile (runs of consecutive atoms)
 constexpr int kMaxRowAtoms = 32;      // atoms of one row cluster
 constexpr int kMaxColAtoms = 16;      // atoms of one column cluster
 constexpr int kMaxBlocks = kMaxRowAtoms * kMaxColAtoms;  // C blocks of one tile
@@ -91,7 +91,7 @@ constexpr int kTileThreads = 32 * (kEpiWarp0 + 4);
 constexpr int kUnits = 32 * (8 + 4);          // 16-byte (row, chunk) copies of a stage and plane
 static_assert(kUnits % kProducers == 0, "units split evenly over the producers");
 constexpr int kTmemCols = 512;
-constexpr int64_t kRowMask = (1 << 25) - 1;  // panel row of an entry (bk in the top 7 bits)
+constexpr int64_t kRowMask = (1 << 25) - 1;  // panel row of an entry (its row count in the top 7 bits)
 // Level accumulators stay exact while (K rows) * S * 127^2 < 2^31.
 constexpr int64_t kMaxKRows = (int64_t)INT_MAX / (kS * 127 * 127);
 constexpr double kFirst = 127.0, kBase = 254.0;
