@@ -49,3 +49,22 @@ def test_context_creation_fails_cleanly_without_gpu():
     from lamb_b200 import gpu
     with pytest.raises(gpu.LambError):
         gpu.Context(0)
+
+
+def test_probe_library_exports_header_and_refuses_bad_arguments():
+    """Every probe declared in lamb_probe.h is exported; the tcgen05 probe
+    refuses an unknown instruction width or a null output before it touches
+    a device."""
+    from lamb_b200 import build
+    lib = ctypes.CDLL(build.build_cuda())
+    names = _declared("lamb_probe.h")
+    assert "lamb_probe_int8_tcgen05_tops" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    f = lib.lamb_probe_int8_tcgen05_tops
+    f.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+    f.restype = ctypes.c_int32
+    out = ctypes.c_double(-1.0)
+    for n in (7, 128, -1):
+        assert lib.lamb_gpu_status_type(f(0, n, 1, ctypes.byref(out))) == 100
+    assert lib.lamb_gpu_status_type(f(0, 0, 1, None)) == 100
