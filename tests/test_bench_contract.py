@@ -27,3 +27,23 @@ def test_reference_arm_other_ranks_idle():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     out = subprocess.run(ARGS, capture_output=True, text=True, timeout=600, cwd=REPO, env=env)
     assert out.returncode == 0 and out.stdout.strip() == ""
+
+
+def test_committed_traffic_summaries():
+    """The DRAM-traffic summaries the bench line reads (small-case ncu
+    captures scaled per workload) are consistent: the headline workload is
+    present, and each scaled figure is the capture's per-unit bytes times the
+    workload's units."""
+    sys.path.insert(0, REPO)
+    import bench
+    for kernel, unit in (("k_stacked", "bytes_per_product"), ("k_tc_tiles", "bytes_per_tensor_op")):
+        with open(os.path.join(REPO, "profiles", f"{kernel}_traffic.json")) as f:
+            d = json.load(f)
+        per = d["per_multiply_bytes"]
+        assert per["water6144_cut8"] > 0 and d[unit] > 0
+        assert bench.committed_traffic(kernel, "water6144_cut8") == per["water6144_cut8"]
+        assert bench.committed_traffic(kernel, "no_such_workload") is None
+        cap = d["capture"]
+        units = cap.get("n_products", cap.get("tensor_ops"))
+        total = cap.get("bytes", cap.get("read_bytes_per_multiply", 0) + cap.get("write_bytes_per_multiply", 0))
+        assert abs(total / units - d[unit]) <= 1e-9 * d[unit]
